@@ -1,0 +1,389 @@
+/*
+ * fdtd_oracle.c -- CPU restatement of AlpineEM's FDTD solver, used ONLY as a
+ * test oracle and as the timed CPU baseline.  It is test infrastructure: the
+ * product (alpineem_b200) never links, loads or calls anything in this
+ * directory.
+ *
+ * What it restates: the single Fortran program `main_fdtd/fdtd_solver.f90`
+ * of DanRich123/AlpineEM -- input parse (:726-1298), derived parameters
+ * (:1305-1812), geometry rasterisation and cell->edge averaging
+ * (:1829-2757), Ga/Gb + Drude coefficients (:2794-3248), CPML and den_*
+ * arrays (:3290-3666), sheet lists and gridded feeds (:3676-3744), the time
+ * loop (:4440-8299) and the finalize/writers (:8338-8807), plus the two
+ * contained functions Inc / E_or_V_1D (:8825-8902).  Statement order and
+ * loop bounds follow the reference; each block cites the lines it restates.
+ *
+ * Build variants (see oracle/Makefile):
+ *   default          FP32 fields and coefficients, standard solver
+ *   -DORACLE_F64     same algorithm in FP64 (the "FP64 oracle")
+ *   -DORACLE_KMAX    constant-k periodic (kmax) variant, complex fields
+ * SPICE co-simulation (use_spice_version) is not restated: it needs
+ * libngspice, which is not part of the path.
+ *
+ * Deliberate, documented deviations from the Fortran binary:
+ *  - far-field bins are accumulated per angle in a fixed order instead of
+ *    with OpenMP/OpenACC atomics (the reference order is unspecified);
+ *  - plane-sum reductions (S-parameter planes) are summed sequentially;
+ *  - two out-of-bounds reads in the reference are given defined values:
+ *    C_inc(0) in the antenna clear run (:8389-8399, read as 0) and the
+ *    gridded-feed normalisation index jj+1 (:4950, read through Fortran's
+ *    column-major aliasing, 0 past the end of the array).
+ * Parity status: pinned end-to-end against the reference's committed example
+ * CSVs through the reference's own post-processor (tests/golden).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <ctype.h>
+#include <stdint.h>
+#include <tgmath.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include <time.h>
+
+#ifdef ORACLE_F64
+typedef double real_t;
+#define RSTRTO(s, e) strtod((s), (e))
+#else
+typedef float real_t;
+#define RSTRTO(s, e) strtof((s), (e))
+#endif
+#define R(x) ((real_t)(x))
+
+#ifdef ORACLE_KMAX
+#ifdef ORACLE_F64
+typedef double _Complex fld_t;
+#else
+typedef float _Complex fld_t;
+#endif
+#define IMAG ((fld_t)I)
+#define RE(z) creal(z)
+#define IM(z) cimag(z)
+#else
+typedef real_t fld_t;
+#define IMAG R(0.0)
+#define RE(z) (z)
+#define IM(z) R(0.0)
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* 1-based Fortran-layout arrays (first index fastest)                       */
+/* ------------------------------------------------------------------------ */
+typedef struct { real_t *p; int n1, n2, n3, n4; } RA;
+typedef struct { fld_t *p; int n1, n2, n3, n4; } FA;
+typedef struct { int *p; int n1, n2, n3, n4; } IA;
+
+#define NEW_ARR(A, T, a, b, c, d)                                             \
+    do {                                                                      \
+        (A).n1 = (a) > 0 ? (a) : 0; (A).n2 = (b) > 0 ? (b) : 0;               \
+        (A).n3 = (c) > 0 ? (c) : 0; (A).n4 = (d) > 0 ? (d) : 0;               \
+        size_t _n = (size_t)(A).n1 * (A).n2 * (A).n3 * (A).n4;                \
+        (A).p = (T *)calloc(_n ? _n : 1, sizeof(T));                          \
+        if (!(A).p) { fprintf(stderr, "oracle: out of memory\n"); exit(3); }  \
+    } while (0)
+#define NEW3(A, T, a, b, c) NEW_ARR(A, T, a, b, c, 1)
+#define NEW2(A, T, a, b) NEW_ARR(A, T, a, b, 1, 1)
+#define NEW1(A, T, a) NEW_ARR(A, T, a, 1, 1, 1)
+#define SIZE_OF(A) ((size_t)(A).n1 * (A).n2 * (A).n3 * (A).n4)
+#define FREE(A) do { free((A).p); (A).p = NULL; } while (0)
+
+#define AT1(a, i) ((a).p[(size_t)((i) - 1)])
+#define AT2(a, i, j) ((a).p[(size_t)((j) - 1) * (a).n1 + (size_t)((i) - 1)])
+#define AT3(a, i, j, k) \
+    ((a).p[((size_t)((k) - 1) * (a).n2 + (size_t)((j) - 1)) * (a).n1 + (size_t)((i) - 1)])
+#define AT4(a, i, j, k, l)                                                          \
+    ((a).p[(((size_t)((l) - 1) * (a).n3 + (size_t)((k) - 1)) * (a).n2 + (size_t)((j) - 1)) * \
+               (a).n1 + (size_t)((i) - 1)])
+
+static void fill_r(RA a, real_t v) { size_t n = SIZE_OF(a); for (size_t q = 0; q < n; q++) a.p[q] = v; }
+
+static void die(const char *msg) {
+    /* the reference stops with STOP "ERROR: ..." */
+    printf("%s\n", msg);
+    exit(2);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Fortran list-directed input, restated for the inputs.txt grammar          */
+/* ------------------------------------------------------------------------ */
+static char **g_lines;
+static int g_nlines, g_cur;
+
+static void load_lines(const char *path) {
+    FILE *f = fopen(path, "rb");
+    if (!f) { fprintf(stderr, "oracle: cannot open %s\n", path); exit(2); }
+    fseek(f, 0, SEEK_END); long n = ftell(f); fseek(f, 0, SEEK_SET);
+    char *buf = (char *)malloc((size_t)n + 2);
+    if (fread(buf, 1, (size_t)n, f) != (size_t)n) { fprintf(stderr, "oracle: read error\n"); exit(2); }
+    buf[n] = '\0'; fclose(f);
+    int cap = 64; g_lines = (char **)malloc(sizeof(char *) * cap); g_nlines = 0;
+    char *s = buf;
+    while (*s) {
+        char *e = strchr(s, '\n');
+        if (e) *e = '\0';
+        size_t L = strlen(s);
+        if (L && s[L - 1] == '\r') s[L - 1] = '\0';
+        if (g_nlines == cap) { cap *= 2; g_lines = (char **)realloc(g_lines, sizeof(char *) * cap); }
+        g_lines[g_nlines++] = s;
+        if (!e) break;
+        s = e + 1;
+    }
+    g_cur = 0;
+}
+
+/* Collect n list-directed tokens starting at a new record; a READ statement
+ * that needs more values continues onto following records and discards the
+ * unread rest of its last record (Fortran semantics). */
+static int next_tokens(int n, char tok[][128]) {
+    int got = 0;
+    while (got < n) {
+        if (g_cur >= g_nlines) { fprintf(stderr, "oracle: unexpected end of input file\n"); exit(2); }
+        char *s = g_lines[g_cur++];
+        while (*s && got < n) {
+            while (*s == ' ' || *s == '\t') s++;
+            if (!*s) break;
+            if (*s == ',') { s++; continue; }
+            int L = 0;
+            if (*s == '\'' || *s == '"') {
+                char q = *s++;
+                while (*s && *s != q && L < 127) tok[got][L++] = *s++;
+                if (*s == q) s++;
+            } else {
+                while (*s && *s != ',' && *s != ' ' && *s != '\t' && L < 127) tok[got][L++] = *s++;
+            }
+            tok[got][L] = '\0';
+            got++;
+        }
+    }
+    return got;
+}
+static void rd_i(int n, int *out) {
+    char t[8][128]; next_tokens(n, t);
+    for (int q = 0; q < n; q++) {
+        char *e; long v = strtol(t[q], &e, 10);
+        if (*e) { fprintf(stderr, "oracle: bad integer '%s'\n", t[q]); exit(2); }
+        out[q] = (int)v;
+    }
+}
+static real_t parse_real(const char *s) {
+    char b[128]; strncpy(b, s, 127); b[127] = 0;
+    for (char *p = b; *p; p++) if (*p == 'd' || *p == 'D') *p = 'E';
+    char *e; real_t v = RSTRTO(b, &e);
+    if (e == b) { fprintf(stderr, "oracle: bad real '%s'\n", s); exit(2); }
+    return v;
+}
+static void rd_r(int n, real_t *out) {
+    char t[8][128]; next_tokens(n, t);
+    for (int q = 0; q < n; q++) out[q] = parse_real(t[q]);
+}
+/* character(len=maxlen) list-directed read: one token, truncated */
+static void rd_s(char *out, int maxlen) {
+    char t[1][128]; next_tokens(1, t);
+    snprintf(out, (size_t)maxlen + 1, "%s", t[0]);
+}
+/* read(1,'(a)') into character(len=maxlen) */
+static void rd_line(char *out, int maxlen) {
+    if (g_cur >= g_nlines) { fprintf(stderr, "oracle: unexpected end of input file\n"); exit(2); }
+    strncpy(out, g_lines[g_cur++], (size_t)maxlen); out[maxlen] = '\0';
+}
+/* adjustl(trim(s)) */
+static void trimlr(char *s) {
+    char *a = s; while (*a == ' ' || *a == '\t') a++;
+    memmove(s, a, strlen(a) + 1);
+    size_t L = strlen(s); while (L && (s[L - 1] == ' ' || s[L - 1] == '\t')) s[--L] = '\0';
+}
+
+/* ------------------------------------------------------------------------ */
+/* Program state (the reference keeps everything global to Program fdtd)     */
+/* ------------------------------------------------------------------------ */
+static const real_t c0 = R(299792458.0);
+static const real_t mu_0 = R(1.25663706E-6);
+static const real_t ep_0 = R(8.85418782E-12);
+static const real_t pi = R(3.14159265358979323846);
+static const int m_pml = 3, ma_pml = 1;
+
+static real_t spread, t_spread, del_t, min_steps;
+static real_t del_x, del_y, del_z;
+static int nxPML_1 = 11, nxPML_2 = 11, nyPML_1 = 11, nyPML_2 = 11, nzPML_1 = 11, nzPML_2 = 11;
+static real_t sig_x_max, sig_y_max, sig_z_max, alpha_x_max, alpha_y_max, alpha_z_max;
+static real_t kappa_x_max, kappa_y_max, kappa_z_max;
+static real_t DA, DB;
+static int xlow, xhigh, ylow, yhigh, zlow, zhigh;
+static int buffer_cells = 3;
+static real_t WHx, WHy, WHz, WEx, WEy, WEz;
+static real_t WHx_m, WHy_m, WHz_m, WEx_m, WEy_m, WEz_m;
+static int x_delay, y_delay, z_delay, x_delay_m, y_delay_m, z_delay_m;
+static real_t sheet_thickness;
+static int port_array_size;
+static int pbc_x, pbc_y, pbc_z;
+static int vid_size1, vid_size2;
+static int ic, jc, kc;
+static int len_ff;
+static real_t r_relay;
+static real_t xlow_wall = 1, ylow_wall = 1, zlow_wall = 1, xhigh_wall = 1, yhigh_wall = 1, zhigh_wall = 1;
+static real_t Mx_mir = 1, My_mir = 1, Mz_mir = 1, Jx_mir = 1, Jy_mir = 1, Jz_mir = 1;
+static real_t x_mir_off, y_mir_off, z_mir_off, use_x_mir, use_y_mir, use_z_mir;
+static int ff_xlow, ff_xhigh, ff_ylow, ff_yhigh, ff_zlow, ff_zhigh;
+static int count_sh_x, count_sh_y, count_sh_z;
+static int plasma_box[3][6]; /* per field component: zmin,zmax,ymin,ymax,xmin,xmax */
+
+static int x_size, y_size, z_size, time_steps, pulse_type;
+static real_t step_x, step_y, step_z, factor_dt, f_center;
+static real_t theta, phi, pol, theta_m, phi_m;
+static int video_on, slice_dir, slice_loc;
+static char filename[31];
+static char export_all[6];
+static int num_materials, num_sheet_materials, num_objects, num_blocks, num_spheres, num_cylinders;
+static int num_sheets_x, num_sheets_y, num_sheets_z, num_ports, num_ff;
+static real_t pw_amp, pw_delay, ant_amp, ant_delay;
+static int exc_port;
+static char excitation_type[16];
+static int is_mirror, mirror_type, mirror_height;
+static int is_plasma, num_poles;
+static char use_bulk[6], bulk_name[51];
+static int sim_bc[6];
+#ifdef ORACLE_KMAX
+static int mode_type, k_direction;
+static real_t k_count_x, k_count_y, k_count_z;
+static real_t k_num_x_exc, k_num_y_exc, k_num_z_exc, f_adj;
+static int k_pl_start_E, k_pl_start_H;
+#endif
+
+static RA materials_properties; /* (num_materials,15,3) */
+static RA sheet_properties;     /* (num_sheet_materials,4,3) */
+static IA blocks, spheres, cylinders, sheets_x, sheets_y, sheets_z;
+static char (*object_type)[16];
+static RA ports;                /* (num_ports,5,4) */
+static char (*gridded_names)[31];
+static RA far_field_angles;     /* (n,2) */
+
+/* fields */
+static FA Ex, Ey, Ez, Hx, Hy, Hz;
+static RA Gax, Gbx, Gay, Gby, Gaz, Gbz;
+static FA J_source_x, J_source_y, J_source_z, Ex_oldt, Ey_oldt, Ez_oldt;
+static RA J_plasma_ax, J_plasma_bx, J_plasma_ay, J_plasma_by, J_plasma_az, J_plasma_bz;
+static FA Voltage, Current, Voltage_out, V_inc, C_inc;
+static FA Ex_video, Ey_video, Ez_video, Hx_video, Hy_video, Hz_video;
+static FA Ex_all, Ey_all, Ez_all, Hx_all, Hy_all, Hz_all;
+static FA incident_w;
+#ifdef ORACLE_KMAX
+static FA E_refl_TE, E_refl_TM, E_trans_TE, E_trans_TM;
+#else
+static FA E_reflected, E_transmitted;
+#endif
+static FA Ex_special, Ey_special, Ez_special;
+static IA x_sheet_list, y_sheet_list, z_sheet_list;
+static RA sheet_sig_x_x, sheet_ep_x_x, sheet_sig_y_y, sheet_ep_y_y, sheet_sig_z_z, sheet_ep_z_z;
+static RA den_ex, den_ey, den_ez, den_hx, den_hy, den_hz;
+static FA psi_Ezx_1, psi_Hyx_1, psi_Ezy_1, psi_Hxy_1, psi_Exz_1, psi_Hyz_1, psi_Eyz_1, psi_Hxz_1;
+static FA psi_Eyx_1, psi_Hzx_1, psi_Exy_1, psi_Hzy_1;
+static FA psi_Ezx_2, psi_Hyx_2, psi_Ezy_2, psi_Hxy_2, psi_Exz_2, psi_Hyz_2, psi_Eyz_2, psi_Hxz_2;
+static FA psi_Eyx_2, psi_Hzx_2, psi_Exy_2, psi_Hzy_2;
+static RA be_x_1, ce_x_1, bh_x_1, ch_x_1, be_x_2, ce_x_2, bh_x_2, ch_x_2;
+static RA be_y_1, ce_y_1, bh_y_1, ch_y_1, be_y_2, ce_y_2, bh_y_2, ch_y_2;
+static RA be_z_1, ce_z_1, bh_z_1, ch_z_1, be_z_2, ce_z_2, bh_z_2, ch_z_2;
+static RA kappah_x_1, kappah_x_2, kappae_x_1, kappae_x_2;
+static RA kappah_y_1, kappah_y_2, kappae_y_1, kappae_y_2;
+static RA kappah_z_1, kappah_z_2, kappae_z_1, kappae_z_2;
+static RA gridded_feed_all; /* (num_ports,4,M1,M2) */
+/* far field */
+static FA My_xlow, Mz_xlow, Jy_xlow, Jz_xlow, My_xlow_o, Mz_xlow_o, Jy_xlow_o, Jz_xlow_o;
+static FA My_xhigh, Mz_xhigh, Jy_xhigh, Jz_xhigh, My_xhigh_o, Mz_xhigh_o, Jy_xhigh_o, Jz_xhigh_o;
+static FA Mx_ylow, Mz_ylow, Jx_ylow, Jz_ylow, Mx_ylow_o, Mz_ylow_o, Jx_ylow_o, Jz_ylow_o;
+static FA Mx_yhigh, Mz_yhigh, Jx_yhigh, Jz_yhigh, Mx_yhigh_o, Mz_yhigh_o, Jx_yhigh_o, Jz_yhigh_o;
+static FA Mx_zlow, My_zlow, Jx_zlow, Jy_zlow, Mx_zlow_o, My_zlow_o, Jx_zlow_o, Jy_zlow_o;
+static FA Mx_zhigh, My_zhigh, Jx_zhigh, Jy_zhigh, Mx_zhigh_o, My_zhigh_o, Jx_zhigh_o, Jy_zhigh_o;
+static FA Wx, Wy, Wz, Ux, Uy, Uz, E_theta_out, E_phi_out;
+static int *data_out_time;
+static FA Ex_ff_pc, Ey_ff_pc, Ez_ff_pc, Hx_ff_pc, Hy_ff_pc, Hz_ff_pc;
+static FILE *full_files[6];
+
+/* ------------------------------------------------------------------------ */
+/* contained functions, ref :8825-8902                                       */
+/* ------------------------------------------------------------------------ */
+#ifndef ORACLE_KMAX
+/* Inc, ref :8825-8842 */
+static inline real_t Inc(real_t w, real_t x, real_t y, real_t z, real_t counter, real_t th, real_t ph,
+                         int xd, int yd, int zd) {
+    real_t tx = sin(th) * cos(ph) * (x - (real_t)xd) * del_x;
+    real_t ty = sin(th) * sin(ph) * (y - (real_t)yd) * del_y;
+    real_t tz = cos(th) * (z - (real_t)zd) * del_z;
+    real_t arg = (t_spread - (counter * del_t) + (R(1.0) / c0) * (tx + ty + tz)) / spread;
+    real_t v = R(0.0);
+    if (pulse_type == 1) v = w * exp(R(-0.5) * (arg * arg));
+    if (pulse_type == 2) v = R(-1.0) * w * arg * exp(R(0.5)) * exp(R(-0.5) * (arg * arg));
+    return v;
+}
+/* E_or_V_1D, ref :8844-8857 */
+static inline real_t E_or_V_1D(real_t amp, real_t tc, real_t posd) {
+    real_t a = (t_spread - ((tc - R(1.0)) * del_t) - R(1.0) / c0 * posd) / spread;
+    real_t v = R(0.0);
+    if (pulse_type == 1) v = amp * exp(R(-0.5) * (a * a));
+    if (pulse_type == 2) v = amp * R(-1.0) * a * exp(R(0.5)) * exp(R(-0.5) * (a * a));
+    return v;
+}
+#else
+/* Inc (kmax), ref :8861-8887 */
+static inline fld_t Inc(real_t w, real_t xf, real_t kyf, real_t dyf, real_t kzf, real_t dzf, real_t fv,
+                        real_t counter, real_t dxf) {
+    real_t a = (t_spread - (counter * del_t) + R(1.0) / c0 * (xf * dxf)) / spread;
+    real_t arg1 = w * exp(R(-0.5) * (a * a));
+    fld_t arg2 = exp(IMAG * R(2.0) * pi * fv * ((counter * del_t) + R(1.0) / c0 * (xf * dxf)) -
+                     R(1.0) * IMAG * (kyf * dyf + kzf * dzf));
+    return arg1 * arg2;
+}
+/* E_or_V_1D (kmax), ref :8889-8902 */
+static inline fld_t E_or_V_1D(real_t amp, real_t tc, real_t posd) {
+    real_t a = (t_spread - ((tc - R(1.0)) * del_t) - R(1.0) / c0 * posd) / spread;
+    return amp * exp(R(-0.5) * (a * a)) *
+           exp(IMAG * R(2.0) * pi * f_adj * ((tc - R(1.0)) * del_t - R(1.0) / c0 * posd));
+}
+#endif
+
+#include "oracle_parse.inc"
+#include "oracle_setup.inc"
+#include "oracle_loop.inc"
+#include "oracle_output.inc"
+
+int main(int argc, char **argv) {
+    if (argc < 2) { fprintf(stderr, "usage: %s inputs.txt\n", argv[0]); return 2; }
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    printf("Reading in the inputs file and setting up the simulation...\n");
+    parse_inputs(argv[1]);
+    setup_all();
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    printf("Setup is finished. Time to complete was %.3f seconds.\n",
+           (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec));
+    printf("Starting main FDTD algorithm...\n");
+    int max_steps = time_steps;
+    const char *lim = getenv("ORACLE_MAX_STEPS"); /* bounded CPU-baseline samples */
+    if (lim && atoi(lim) > 0 && atoi(lim) < max_steps) max_steps = atoi(lim);
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (int counter = 1; counter <= max_steps; counter++) time_step(counter);
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    double secs = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+    printf("Finished main FDTD algorithm. Time to complete was %.3f seconds.\n", secs);
+    printf("Average of %.2f Mcells per second.\n",
+           1.0e-6 * (double)(x_size - 1) * (y_size - 1) * (z_size - 1) * max_steps / secs);
+    const char *tf = getenv("ORACLE_TIMING_FILE");
+    if (tf) {
+        FILE *f = fopen(tf, "w");
+        if (f) {
+            int thr = 1;
+#ifdef _OPENMP
+            thr = omp_get_max_threads();
+#endif
+            fprintf(f, "{\"steps\": %d, \"seconds\": %.6f, \"cells\": %.0f, \"threads\": %d}\n", max_steps, secs,
+                    (double)(x_size - 1) * (y_size - 1) * (z_size - 1), thr);
+            fclose(f);
+        }
+    }
+    if (max_steps == time_steps) {
+        printf("Post processing some data...\n");
+        finalize_and_write();
+    }
+    dump_fields_if_requested();
+    return 0;
+}
