@@ -1,0 +1,179 @@
+"""alpineem_b200 -- B200 (sm_100a) implementation of AlpineEM's FDTD core.
+
+The reference drives its solver as an executable: ``master.py`` writes a
+positional ``inputs.txt`` and runs ``./<solver> inputs.txt``
+(main_fdtd/master.py:438-441); ``post_processor.py`` then reads the
+``<name>.dat`` it leaves behind.  This package offers the same solver as
+
+* ``_lib/FDTD-B200`` -- drop-in executable (set ``solver='<path>/FDTD-B200'``
+  in master.py; ``FDTD-B200-kmax`` or ``--kmax`` for the constant-k build);
+* :class:`Simulation` -- the C ABI of ``libalpineem_b200.so`` through ctypes,
+  for stepping a run and reading its series and fields from Python;
+* :func:`run_deck` -- one call equivalent to the executable.
+
+There is no CPU fallback: importing works without a GPU, but creating a
+simulation needs the CUDA library and a device, and fails loudly otherwise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libalpineem_b200.so")
+EXE_PATH = os.path.join(_HERE, "_lib", "FDTD-B200")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "alpineem_b200.h")
+
+STANDARD, KMAX = 0, 1
+SERIES = {"incident": 0, "reflected": 1, "transmitted": 2, "reflected_tm": 3, "transmitted_tm": 4,
+          "port_voltage": 5, "e_theta": 6, "e_phi": 7}
+FIELDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
+
+_lib = None
+
+
+class AemError(RuntimeError):
+    """A failing call of the solver library (message from aem_last_error)."""
+
+
+def load_library():
+    """Load libalpineem_b200.so (built in-tree by alpineem_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libalpineem_b200.so is not built (%s); run `python alpineem_b200/build.py`" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    h = ctypes.c_void_p
+    lib.aem_version.restype = ctypes.c_int
+    lib.aem_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(h)]
+    lib.aem_run.argtypes = [h, ctypes.c_int]
+    lib.aem_steps.argtypes = [h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.aem_synchronize.argtypes = [h]
+    lib.aem_write_outputs.argtypes = [h]
+    lib.aem_get_series.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    lib.aem_get_field.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double)]
+    lib.aem_grid.argtypes = [h, ctypes.POINTER(ctypes.c_int)]
+    lib.aem_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_size_t)]
+    lib.aem_last_error.argtypes = [h]
+    lib.aem_last_error.restype = ctypes.c_char_p
+    lib.aem_destroy.argtypes = [h]
+    _lib = lib
+    return lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+class Simulation:
+    """One solver run on the current CUDA device.
+
+    ``Simulation("inputs.txt").run_all()`` reproduces ``./FDTD inputs.txt``
+    of the reference: it writes ``<name>_geometry.bin`` at creation and
+    ``<name>.dat`` (and video files when the deck asks) on
+    :meth:`write_outputs`.  Output files go to ``outdir`` (default: current
+    directory, like the reference executable).
+    """
+
+    def __init__(self, inputs_path, kmax=False, outdir=None):
+        self._lib = load_library()
+        self._h = ctypes.c_void_p()
+        rc = self._lib.aem_create_from_file(os.fsencode(inputs_path), KMAX if kmax else STANDARD,
+                                            os.fsencode(outdir) if outdir else None, ctypes.byref(self._h))
+        if rc != 0:
+            raise AemError(self._lib.aem_last_error(None).decode())
+        self.kmax = kmax
+
+    def _check(self, rc):
+        if rc < 0:
+            raise AemError(self._lib.aem_last_error(self._h).decode())
+        return rc
+
+    @property
+    def steps(self):
+        d, t = ctypes.c_int(), ctypes.c_int()
+        self._lib.aem_steps(self._h, ctypes.byref(d), ctypes.byref(t))
+        return d.value, t.value
+
+    @property
+    def grid(self):
+        g = (ctypes.c_int * 3)()
+        self._lib.aem_grid(self._h, g)
+        return tuple(g)
+
+    @property
+    def device_bytes(self):
+        b = ctypes.c_size_t()
+        self._lib.aem_device_bytes(self._h, ctypes.byref(b))
+        return b.value
+
+    def run(self, nsteps):
+        self._check(self._lib.aem_run(self._h, int(nsteps)))
+
+    def synchronize(self):
+        self._check(self._lib.aem_synchronize(self._h))
+
+    def run_all(self, write=True):
+        done, total = self.steps
+        self.run(total - done)
+        self.synchronize()
+        if write:
+            self.write_outputs()
+        return self
+
+    def write_outputs(self):
+        self._check(self._lib.aem_write_outputs(self._h))
+
+    def series(self, kind, index=0):
+        """A time series of the finished run (complex for kmax)."""
+        k = SERIES[kind] if isinstance(kind, str) else int(kind)
+        n = self.steps[1]
+        re, im = np.zeros(n), np.zeros(n)
+        m = self._check(self._lib.aem_get_series(self._h, k, int(index), _dptr(re), _dptr(im), n))
+        return (re[:m] + 1j * im[:m]) if self.kmax else re[:m]
+
+    def field(self, comp):
+        """Final field component in the reference's layout, shape (nz, ny, nx) of F-order (x fastest)."""
+        c = FIELDS[comp] if isinstance(comp, str) else int(comp)
+        dims = (ctypes.c_int * 3)()
+        self._check(self._lib.aem_get_field(self._h, c, dims, None, None))
+        n = dims[0] * dims[1] * dims[2]
+        re, im = np.zeros(n), np.zeros(n)
+        self._check(self._lib.aem_get_field(self._h, c, dims, _dptr(re), _dptr(im)))
+        shape = (dims[2], dims[1], dims[0])
+        out = re.reshape(shape)
+        return out + 1j * im.reshape(shape) if self.kmax else out
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.aem_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_deck(inputs_path, kmax=False, outdir=None):
+    """Run a whole deck and write the reference's output files."""
+    with Simulation(inputs_path, kmax=kmax, outdir=outdir) as sim:
+        sim.run_all()
+
+
+def exported_symbols():
+    """Function names declared in include/alpineem_b200.h."""
+    import re
+    with open(HEADER_PATH) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"\b(aem_[a-z_]+)\s*\(", txt)))

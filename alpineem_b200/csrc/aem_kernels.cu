@@ -1,0 +1,492 @@
+// aem_kernels.cu -- the per-step field updates on sm_100a.
+//
+// Two bandwidth-bound kernels per time step, each a 2.5D march along z over
+// (32 x 8)-thread column tiles:
+//   k_update_h : H^{n+1/2} from E^n  -- bulk curl (fdtd_solver.f90:4442-4484),
+//                Smith-Maloney sheet terms (:4486-4554), TF/SF or kmax plane
+//                source (:4558-4794), CPML psi (:5227-5375), PBC (:5377-5433)
+//                by periodic indexing
+//   k_update_e : E^{n+1} from H     -- bulk update with per-cell material IDs
+//                (:5667-5710), sheet sub-cell field (:5712-5780), Drude ADE
+//                (:5782-5854), TF/SF or kmax plane source (:5857-6117), CPML
+//                psi (:6522-6670), PBC (:6672-6806) by periodic indexing
+// The ports, far-field and output taps run as small kernels in
+// aem_aux.cu.  Every correction is applied in the reference's statement
+// order; built with -fmad=false so the FP32 results round like the
+// reference's expressions.
+#include "aem_dev.cuh"
+#include "aem_kernels.h"
+
+namespace aem {
+
+template <typename T>
+__device__ inline T ld(const void* base, long long i) {
+    return reinterpret_cast<const T*>(base)[i];
+}
+template <typename T>
+__device__ inline void st(void* base, long long i, T v) {
+    reinterpret_cast<T*>(base)[i] = v;
+}
+
+// read a neighbour that may sit across a periodic boundary (Bloch phase
+// exp(-ikL) when stepping past the last position)
+template <typename T>
+__device__ inline T ld_up(const AemParams& P, const void* base, long long i, bool wrapped, int axis) {
+    T v = ld<T>(base, i);
+    return wrapped ? bloch<T>(v, P, axis, -1) : v;
+}
+template <typename T>
+__device__ inline T ld_dn(const AemParams& P, const void* base, long long i, bool wrapped, int axis) {
+    T v = ld<T>(base, i);
+    return wrapped ? bloch<T>(v, P, axis, +1) : v;
+}
+
+// CPML psi update and add-on, ref :5234-5236 (H) / :6529-6531 (E)
+template <typename T>
+__device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T diff, float dl, long long q) {
+    T old = ld<T>(psi, q);
+    T nw = b * old + c * diff / dl;
+    st<T>(psi, q, nw);
+    return nw;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemParams P, int counter) {
+    const int px = blockIdx.x * 32 + threadIdx.x;
+    const int py = blockIdx.y * 8 + threadIdx.y;
+    // H is updated on reference indices 1..N-1 of every axis (all positions
+    // of a periodic axis)
+    const int hx = P.per[0] ? P.SX - 1 : P.SX - 2;
+    const int hy = P.per[1] ? P.SY - 1 : P.SY - 2;
+    const int hz = P.per[2] ? P.SZ - 1 : P.SZ - 2;
+    if (px > hx || py > hy) return;
+    const void *Ex = P.E[0], *Ey = P.E[1], *Ez = P.E[2];
+    void *Hx = P.H[0], *Hy = P.H[1], *Hz = P.H[2];
+    bool wx, wy;
+    const int pxn = wrap_up(P, 0, px, P.SX, &wx);
+    const int pyn = wrap_up(P, 1, py, P.SY, &wy);
+    const int i = px + 1, j = py + 1;
+    const float DB = P.DB;
+    const float dhx = P.den_h[0][i - 1], dhy = P.den_h[1][j - 1];
+    const float cntH = (float)counter - 1.0f;
+    // this column's CPML membership along x and y
+    const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0;
+    const int qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
+    const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0;
+    const int qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+
+    for (int pz = 0; pz <= hz; pz++) {
+        bool wz;
+        const int pzn = wrap_up(P, 2, pz, P.SZ, &wz);
+        const int k = pz + 1;
+        const long long c = lin(P, px, py, pz);
+        const float dhz = P.den_h[2][k - 1];
+        const T ex = ld<T>(Ex, c), ey = ld<T>(Ey, c), ez = ld<T>(Ez, c);
+        const T ex_jp = ld_up<T>(P, Ex, lin(P, px, pyn, pz), wy, 1);
+        const T ex_kp = ld_up<T>(P, Ex, lin(P, px, py, pzn), wz, 2);
+        const T ey_ip = ld_up<T>(P, Ey, lin(P, pxn, py, pz), wx, 0);
+        const T ey_kp = ld_up<T>(P, Ey, lin(P, px, py, pzn), wz, 2);
+        const T ez_ip = ld_up<T>(P, Ez, lin(P, pxn, py, pz), wx, 0);
+        const T ez_jp = ld_up<T>(P, Ez, lin(P, px, pyn, pz), wy, 1);
+
+        // bulk, ref :4448-4479 (DA = 1)
+        T hxv = ld<T>(Hx, c) + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
+        T hyv = ld<T>(Hy, c) + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
+        T hzv = ld<T>(Hz, c) + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
+
+        // Smith-Maloney sheets, ref :4486-4554
+        for (int s = 0; s < P.nsheet; s++) {
+            const AemSheetPlane& S = P.sheet[s];
+            const int pn = S.axis == 0 ? px : S.axis == 1 ? py : pz;
+            if (pn != S.pos) continue;  // S.pos is a storage position
+            const float f = DB * (P.sheet_thick / P.del[S.axis]);
+            if (S.axis == 0) {
+                const long long q = (long long)pz * S.pa + py;
+                if (!S.nmask[q]) continue;
+                const T es = ld<T>(S.es, q);
+                const T es_kp = ld_up<T>(P, S.es, (long long)pzn * S.pa + py, wz, 2);
+                const T es_jp = ld_up<T>(P, S.es, (long long)pz * S.pa + pyn, wy, 1);
+                hyv = hyv + f * ((ex_kp - ex + es - es_kp) * dhz);
+                hzv = hzv + f * ((ex - ex_jp + es_jp - es) * dhy);
+            } else if (S.axis == 1) {
+                const long long q = (long long)pz * S.pa + px;
+                if (!S.nmask[q]) continue;
+                const T es = ld<T>(S.es, q);
+                const T es_kp = ld_up<T>(P, S.es, (long long)pzn * S.pa + px, wz, 2);
+                const T es_ip = ld_up<T>(P, S.es, (long long)pz * S.pa + pxn, wx, 0);
+                hxv = hxv + f * (ey - ey_kp + es_kp - es) * dhz;
+                hzv = hzv + f * ((ey_ip - ey - es_ip + es) * dhx);
+            } else {
+                const long long q = (long long)py * S.pa + px;
+                if (!S.nmask[q]) continue;
+                const T es = ld<T>(S.es, q);
+                const T es_jp = ld_up<T>(P, S.es, (long long)pyn * S.pa + px, wy, 1);
+                const T es_ip = ld_up<T>(P, S.es, (long long)py * S.pa + pxn, wx, 0);
+                hxv = hxv + f * (ez_jp - ez - es_jp + es) * dhy;
+                hyv = hyv + f * ((ez - ez_ip + es_ip - es) * dhx);
+            }
+        }
+
+        // incident fields on H
+        if constexpr (sizeof(T) == sizeof(float)) {
+            if (P.tfsf_on) {  // TF/SF faces, ref :4627-4794 (incident then mirrored)
+                const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
+                for (int m = 0; m <= P.mirror_on; m++) {
+                    const float wEx = P.WE[m][0], wEy = P.WE[m][1], wEz = P.WE[m][2];
+                    if (!P.per[1]) {
+                        const float cf_ = P.coef_h[1];
+                        if (j == yl - 1 || j == yh) {
+                            const float yy = (float)(j == yh ? yh : yl), w = j == yh ? P.wall_hi[1] : P.wall_lo[1];
+                            const float sg = j == yh ? 1.0f : -1.0f;
+                            if (k >= zl && k <= zh && i >= xl && i <= xh - 1 + P.per[0])
+                                hzv = sg > 0 ? hzv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w
+                                             : hzv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w;
+                            if (k >= zl && k <= zh - 1 + P.per[2] && i >= xl && i <= xh)
+                                hxv = sg > 0 ? hxv - cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w
+                                             : hxv + cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w;
+                        }
+                    }
+                    if (!P.per[2]) {
+                        const float cf_ = P.coef_h[2];
+                        if (k == zl - 1 || k == zh) {
+                            const float zz = (float)(k == zh ? zh : zl), w = k == zh ? P.wall_hi[2] : P.wall_lo[2];
+                            const bool hiface = k == zh;
+                            if (j >= yl && j <= yh && i >= xl && i <= xh - 1 + P.per[0])
+                                hyv = hiface ? hyv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w
+                                             : hyv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w;
+                            if (j >= yl && j <= yh - 1 + P.per[1] && i >= xl && i <= xh)
+                                hxv = hiface ? hxv + cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w
+                                             : hxv - cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w;
+                        }
+                    }
+                    if (!P.per[0]) {
+                        const float cf_ = P.coef_h[0];
+                        if (i == xl - 1 || i == xh) {
+                            const float xx = (float)(i == xh ? xh : xl), w = i == xh ? P.wall_hi[0] : P.wall_lo[0];
+                            const bool hiface = i == xh;
+                            if (k >= zl && k <= zh && j >= yl && j <= yh - 1 + P.per[1])
+                                hzv = hiface ? hzv - cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w
+                                             : hzv + cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w;
+                            if (k >= zl && k <= zh - 1 + P.per[2] && j >= yl && j <= yh)
+                                hyv = hiface ? hyv + cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w
+                                             : hyv - cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w;
+                        }
+                    }
+                }
+            }
+        } else {
+            if (P.kmax_mode_TE) {  // kmax TE plane on H, ref :4562-4624
+                const int a = P.kmax_src_axis;
+                const int ia = a == 0 ? i : a == 1 ? j : k;
+                if (ia == P.k_pl_H) {
+                    const float cf_ = P.coef_h[a];
+                    const int lo0 = P.lo[0], hi0 = P.hi[0], lo1 = P.lo[1], hi1 = P.hi[1], lo2 = P.lo[2], hi2 = P.hi[2];
+                    const float* kc = P.kcnt;
+                    const float* kn = P.knum;
+                    if (a == 0 && k >= lo2 && k <= hi2 && j >= lo1 && j <= hi1) {
+                        hzv = hzv + cf_ * d_inc_k(P, P.WE[0][1], 0.0f, kc[1], ((float)j + 0.5f) * P.del[1], kc[2], (float)k * P.del[2], cntH, P.del[0]) * kn[2];
+                        hyv = hyv + cf_ * d_inc_k(P, P.WE[0][2], 0.0f, kc[1], (float)j * P.del[1], kc[2], ((float)k + 0.5f) * P.del[2], cntH, P.del[0]) * kn[1];
+                    }
+                    if (a == 1 && k >= lo2 && k <= hi2 && i >= lo0 && i <= hi0) {
+                        hzv = hzv + cf_ * d_inc_k(P, P.WE[0][0], 0.0f, kc[0], ((float)i + 0.5f) * P.del[0], kc[2], (float)k * P.del[2], cntH, P.del[1]) * kn[2];
+                        hxv = hxv + cf_ * d_inc_k(P, P.WE[0][2], 0.0f, kc[0], (float)i * P.del[0], kc[2], ((float)k + 0.5f) * P.del[2], cntH, P.del[1]) * kn[0];
+                    }
+                    if (a == 2 && j >= lo1 && j <= hi1 && i >= lo0 && i <= hi0) {
+                        hxv = hxv + cf_ * d_inc_k(P, P.WE[0][1], 0.0f, kc[1], ((float)j + 0.5f) * P.del[1], kc[0], (float)i * P.del[0], cntH, P.del[2]) * kn[0];
+                        hyv = hyv + cf_ * d_inc_k(P, P.WE[0][0], 0.0f, kc[1], (float)j * P.del[1], kc[0], ((float)i + 0.5f) * P.del[0], cntH, P.del[2]) * kn[1];
+                    }
+                }
+            }
+        }
+
+        // CPML on H, ref :5227-5375: Hx (y then z), Hy (x then z), Hz (x then y)
+        {
+            const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0;
+            const int qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
+            if (qy_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+            if (qz_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qz_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qy_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+        }
+        st<T>(Hx, c, hxv);
+        st<T>(Hy, c, hyv);
+        st<T>(Hz, c, hzv);
+    }
+}
+
+// Material coefficients of one E edge: sheet override, index-1 vacuum
+// default, uniform-neighbourhood table or the reference's 4-cell average.
+struct EdgeCoef {
+    float ga, gb;
+    float ja[AEM_MAX_POLES], jb[AEM_MAX_POLES];
+};
+
+__device__ inline void edge_coef(const AemParams& P, int c, int px, int py, int pz, int pxd, int pyd, int pzd,
+                                 bool unaveraged, EdgeCoef& o) {
+    int id[4];
+    if (unaveraged) {
+        id[0] = id[1] = id[2] = id[3] = 0;
+    } else {
+        // four cells around the edge, ref :2516-2527
+        const uint8_t* C = P.cell;
+        id[0] = C[lin(P, px, py, pz)];
+        if (c == 0) { id[1] = C[lin(P, px, pyd, pz)]; id[2] = C[lin(P, px, py, pzd)]; id[3] = C[lin(P, px, pyd, pzd)]; }
+        else if (c == 1) { id[1] = C[lin(P, pxd, py, pz)]; id[2] = C[lin(P, px, py, pzd)]; id[3] = C[lin(P, pxd, py, pzd)]; }
+        else { id[1] = C[lin(P, pxd, py, pz)]; id[2] = C[lin(P, px, pyd, pz)]; id[3] = C[lin(P, pxd, pyd, pz)]; }
+    }
+    if (id[0] == id[1] && id[0] == id[2] && id[0] == id[3]) {
+        const AemUniformCoef& u = P.ucoef[id[0]];
+        o.ga = u.ga[c];
+        o.gb = u.gb[c];
+        for (int p = 0; p < P.npoles; p++) { o.ja[p] = u.ja[p][c]; o.jb[p] = u.jb[p][c]; }
+        return;
+    }
+    const AemMaterial *m0 = P.mat + id[0], *m1 = P.mat + id[1], *m2 = P.mat + id[2], *m3 = P.mat + id[3];
+    const float e = (m0->eps[c] + m1->eps[c] + m2->eps[c] + m3->eps[c]) / 4.0f;
+    const float s = (m0->sig[c] + m1->sig[c] + m2->sig[c] + m3->sig[c]) / 4.0f;
+    float tp = 0.0f;
+    for (int p = 0; p < P.npoles; p++) {
+        const float w = (m0->wp[p][c] + m1->wp[p][c] + m2->wp[p][c] + m3->wp[p][c]) / 4.0f;
+        const float g = (m0->gam[p][c] + m1->gam[p][c] + m2->gam[p][c] + m3->gam[p][c]) / 4.0f;
+        o.ja[p] = d_ja(g, P.dt);
+        o.jb[p] = d_jb(w, g, P.dt);
+    }
+    for (int p = 0; p < P.npoles; p++) tp = tp + o.jb[p];
+    o.ga = d_ga(s + tp, e, P.dt);
+    o.gb = d_gb(s + tp, e, P.dt);
+}
+
+// sheet-plane Ga/Gb override of E component c at this position, if any
+__device__ inline bool sheet_override(const AemParams& P, int c, int px, int py, int pz, float* ga, float* gb) {
+    for (int s = 0; s < P.nsheet; s++) {
+        const AemSheetPlane& S = P.sheet[s];
+        if (S.axis == c) continue;
+        const int pn = S.axis == 0 ? px : S.axis == 1 ? py : pz;
+        if (pn != S.pos) continue;
+        const int ua = S.axis == 0 ? 1 : 0;
+        const int pa = ua == 0 ? px : py;
+        const int pb = S.axis == 2 ? py : pz;
+        const long long q = (long long)pb * S.pa + pa;
+        const int bit = c == ua ? 1 : 2;
+        if (!(S.tmask[q] & bit)) continue;
+        *ga = bit == 1 ? S.ga1[q] : S.ga2[q];
+        *gb = bit == 1 ? S.gb1[q] : S.gb2[q];
+        return true;
+    }
+    return false;
+}
+
+// Drude ADE of one E edge inside its bounding box, ref :5794-5802
+template <typename T>
+__device__ inline T drude_update(const AemParams& P, int c, int px, int py, int pz, T e_new, T e_old, float gb,
+                                 const EdgeCoef& co) {
+    const int ox = P.jorg[c][0], oy = P.jorg[c][1], oz = P.jorg[c][2];
+    const int nx = P.jext[c][0], ny = P.jext[c][1], nz = P.jext[c][2];
+    const int lx = px - ox, ly = py - oy, lz = pz - oz;
+    if (lx < 0 || ly < 0 || lz < 0 || lx >= nx || ly >= ny || lz >= nz) return e_new;
+    void* J = P.jsrc[c];
+    const long long vol = (long long)nx * ny * nz, base = ((long long)lz * ny + ly) * nx + lx;
+    T t = zero<T>();
+    for (int p = 0; p < P.npoles; p++) t = t + (1.0f + co.ja[p]) * ld<T>(J, p * vol + base);
+    const T e = e_new - gb * t / 2.0f;
+    for (int p = 0; p < P.npoles; p++)
+        st<T>(J, p * vol + base, co.ja[p] * ld<T>(J, p * vol + base) + co.jb[p] * (e + e_old));
+    return e;
+}
+
+__device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk) {
+    const int* b = P.dbox[c];
+    return rk >= b[0] && rk <= b[1] && rj >= b[2] && rj <= b[3] && ri >= b[4] && ri <= b[5];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemParams P, int counter) {
+    const int px = blockIdx.x * 32 + threadIdx.x;
+    const int py = blockIdx.y * 8 + threadIdx.y;
+    if (px >= P.SX || py >= P.SY) return;
+    const void *Hx = P.H[0], *Hy = P.H[1], *Hz = P.H[2];
+    void *Ex = P.E[0], *Ey = P.E[1], *Ez = P.E[2];
+    // update ranges, ref :5670-5702: the normal component covers reference
+    // indices 1..N-1 of its own axis, tangential axes 2..N-1 (walls stay 0)
+    auto upd = [&](int a, int p, bool normal) {
+        const int S = a == 0 ? P.SX : a == 1 ? P.SY : P.SZ;
+        if (P.per[a]) return true;
+        return normal ? (p <= S - 2) : (p >= 1 && p <= S - 2);
+    };
+    const bool ex_xy = upd(0, px, true) && upd(1, py, false);
+    const bool ey_xy = upd(0, px, false) && upd(1, py, true);
+    const bool ez_xy = upd(0, px, false) && upd(1, py, false);
+    if (!ex_xy && !ey_xy && !ez_xy) return;
+    bool wxd, wyd;
+    int pxd = wrap_dn(P, 0, px, P.SX, &wxd);
+    int pyd = wrap_dn(P, 1, py, P.SY, &wyd);
+    if (pxd < 0) pxd = 0;  // only read by components not updated here
+    if (pyd < 0) pyd = 0;
+    const int i = px + 1, j = py + 1;
+    const float dex = P.den_e[0][i - 1], dey = P.den_e[1][j - 1];
+    const float cntE = (float)counter - 0.5f;
+    // representative reference indices for bound tests (periodic axes)
+    const int rix_t = rep_idx(P, 0, px, true), riy_t = rep_idx(P, 1, py, true);
+    const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
+    const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
+    const bool x_unavg = !P.per[0] && i == 1, y_unavg = !P.per[1] && j == 1;
+
+    for (int pz = 0; pz < P.SZ; pz++) {
+        const bool ex_u = ex_xy && upd(2, pz, false), ey_u = ey_xy && upd(2, pz, false), ez_u = ez_xy && upd(2, pz, true);
+        if (!ex_u && !ey_u && !ez_u) continue;
+        bool wzd;
+        int pzd = wrap_dn(P, 2, pz, P.SZ, &wzd);
+        if (pzd < 0) pzd = 0;
+        const int k = pz + 1;
+        const int riz_t = rep_idx(P, 2, pz, true);
+        const float dez = P.den_e[2][k - 1];
+        const bool unavg = x_unavg || y_unavg || (!P.per[2] && k == 1);
+        const long long c = lin(P, px, py, pz);
+        const T hx = ld<T>(Hx, c), hy = ld<T>(Hy, c), hz = ld<T>(Hz, c);
+        const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
+
+        for (int comp = 0; comp < 3; comp++) {
+            if ((comp == 0 && !ex_u) || (comp == 1 && !ey_u) || (comp == 2 && !ez_u)) continue;
+            void* Ec = P.E[comp];
+            // curl of H, ref :5673-5705
+            T d1, d2;   // the two difference terms (second minus first neighbour as in the reference)
+            float den1, den2;
+            if (comp == 0) {
+                const T hz_jm = ld_dn<T>(P, Hz, lin(P, px, pyd, pz), wyd, 1);
+                const T hy_km = ld_dn<T>(P, Hy, lin(P, px, py, pzd), wzd, 2);
+                d1 = hz - hz_jm; den1 = dey; d2 = hy_km - hy; den2 = dez;
+            } else if (comp == 1) {
+                const T hz_im = ld_dn<T>(P, Hz, lin(P, pxd, py, pz), wxd, 0);
+                const T hx_km = ld_dn<T>(P, Hx, lin(P, px, py, pzd), wzd, 2);
+                d1 = hz_im - hz; den1 = dex; d2 = hx - hx_km; den2 = dez;
+            } else {
+                const T hy_im = ld_dn<T>(P, Hy, lin(P, pxd, py, pz), wxd, 0);
+                const T hx_jm = ld_dn<T>(P, Hx, lin(P, px, pyd, pz), wyd, 1);
+                d1 = hy - hy_im; den1 = dex; d2 = hx_jm - hx; den2 = dey;
+            }
+            const T curl = d1 * den1 + d2 * den2;
+            EdgeCoef co;
+            edge_coef(P, comp, px, py, pz, pxd, pyd, pzd, unavg, co);
+            float ga = co.ga, gb = co.gb;
+            if (P.nsheet) sheet_override(P, comp, px, py, pz, &ga, &gb);
+            const T eold = ld<T>(Ec, c);
+            T e = ga * eold + gb * curl;
+
+            // sheet sub-cell field of the normal component, ref :5714-5780
+            for (int s = 0; s < P.nsheet; s++) {
+                const AemSheetPlane& S = P.sheet[s];
+                if (S.axis != comp) continue;
+                const int pn = comp == 0 ? px : comp == 1 ? py : pz;
+                if (pn != S.pos) continue;
+                const int pa = comp == 0 ? py : px, pb = comp == 2 ? py : pz;
+                const long long q = (long long)pb * S.pa + pa;
+                if (!S.nmask[q]) continue;
+                st<T>(S.es, q, S.sa[q] * ld<T>(S.es, q) + S.sb[q] * curl);
+            }
+            // representative indices of this component
+            const int ri = comp == 0 ? px + 1 : rix_t, rj = comp == 1 ? py + 1 : riy_t, rk = comp == 2 ? pz + 1 : riz_t;
+            if (P.has_drude && in_box(P, comp, ri, rj, rk)) e = drude_update<T>(P, comp, px, py, pz, e, eold, gb, co);
+
+            if constexpr (sizeof(T) == sizeof(float)) {
+                if (P.tfsf_on) {  // TF/SF faces, ref :5950-6117
+                    const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
+                    const int pbx = P.per[0], pby = P.per[1], pbz = P.per[2];
+                    for (int m = 0; m <= P.mirror_on; m++) {
+                        const float wHx = P.WH[m][0], wHy = P.WH[m][1], wHz = P.WH[m][2];
+                        const float cy = P.coef_e[1], cz = P.coef_e[2], cx = P.coef_e[0];
+                        if (comp == 0) {
+                            if (!pby && (rj == yl || rj == yh) && rk >= zl + pbz && rk <= zh && ri >= xl && ri <= xh - 1 + pbx) {
+                                if (rj == yl) e = e - cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yl - 0.5f, (float)rk, cntE) * P.wall_lo[1];
+                                else e = e + cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yh + 0.5f, (float)rk, cntE) * P.wall_hi[1];
+                            }
+                            if (!pbz && (rk == zl || rk == zh) && rj >= yl + pby && rj <= yh && ri >= xl && ri <= xh - 1 + pbx) {
+                                if (rk == zl) e = e + cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zl - 0.5f, cntE) * P.wall_lo[2];
+                                else e = e - cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zh + 0.5f, cntE) * P.wall_hi[2];
+                            }
+                        } else if (comp == 1) {
+                            if (!pbz && (rk == zl || rk == zh) && rj >= yl && rj <= yh - 1 + pby && ri >= xl + pbx && ri <= xh) {
+                                if (rk == zl) e = e - cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zl - 0.5f, cntE) * P.wall_lo[2];
+                                else e = e + cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zh + 0.5f, cntE) * P.wall_hi[2];
+                            }
+                            if (!pbx && (ri == xl || ri == xh) && rk >= zl + pbz && rk <= zh && rj >= yl && rj <= yh - 1 + pby) {
+                                if (ri == xl) e = e + cx * d_inc(P, m, wHz, (float)xl - 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_lo[0];
+                                else e = e - cx * d_inc(P, m, wHz, (float)xh + 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_hi[0];
+                            }
+                        } else {
+                            if (!pby && (rj == yl || rj == yh) && rk >= zl && rk <= zh - 1 + pbz && ri >= xl + pbx && ri <= xh) {
+                                if (rj == yl) e = e + cy * d_inc(P, m, wHx, (float)ri, (float)yl - 0.5f, (float)rk + 0.5f, cntE) * P.wall_lo[1];
+                                else e = e - cy * d_inc(P, m, wHx, (float)ri, (float)yh + 0.5f, (float)rk + 0.5f, cntE) * P.wall_hi[1];
+                            }
+                            if (!pbx && (ri == xl || ri == xh) && rk >= zl && rk <= zh - 1 + pbz && rj >= yl + pby && rj <= yh) {
+                                if (ri == xl) e = e - cx * d_inc(P, m, wHy, (float)xl - 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_lo[0];
+                                else e = e + cx * d_inc(P, m, wHy, (float)xh + 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_hi[0];
+                            }
+                        }
+                    }
+                }
+            } else {
+                if (P.kmax_mode_TM) {  // kmax TM plane on E, ref :5861-5947
+                    const int a = P.kmax_src_axis;
+                    const int ia = a == 0 ? ri : a == 1 ? rj : rk;
+                    if (ia == P.k_pl_E) {
+                        const float cf_ = P.coef_e[a];
+                        const float* kc = P.kcnt;
+                        const float* kn = P.knum;
+                        const float fi = (float)(px + 1), fj = (float)(py + 1), fk = (float)(pz + 1);
+                        const float dx = P.del[0], dy = P.del[1], dz = P.del[2];
+                        if (a == 0) {
+                            if (comp == 2 && rk >= 1 && rk <= P.Z - 1 && rj >= 2 && rj <= P.Y - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][1], -0.5f, kc[1], fj * dy, kc[2], (fk + 0.5f) * dz, cntE, dx) * kn[2];
+                            if (comp == 1 && rk >= 2 && rk <= P.Z - 1 && rj >= 1 && rj <= P.Y - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][2], -0.5f, kc[1], (fj + 0.5f) * dy, kc[2], fk * dz, cntE, dx) * kn[1];
+                        } else if (a == 1) {
+                            if (comp == 2 && rk >= 1 && rk <= P.Z - 1 && ri >= 2 && ri <= P.X - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][0], -0.5f, kc[0], fi * dx, kc[2], (fk + 0.5f) * dz, cntE, dy) * kn[2];
+                            if (comp == 0 && rk >= 2 && rk <= P.Z - 1 && ri >= 1 && ri <= P.X - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][2], -0.5f, kc[0], (fi + 0.5f) * dx, kc[2], fk * dz, cntE, dy) * kn[0];
+                        } else {
+                            if (comp == 0 && rj >= 2 && rj <= P.Y - 1 && ri >= 1 && ri <= P.X - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][1], -0.5f, kc[1], fj * dy, kc[0], (fi + 0.5f) * dx, cntE, dz) * kn[0];
+                            if (comp == 1 && rj >= 1 && rj <= P.Y - 1 && ri >= 2 && ri <= P.X - 1)
+                                e = e + cf_ * d_inc_k(P, P.WH[0][0], -0.5f, kc[1], (fj + 0.5f) * dy, kc[0], fi * dx, cntE, dz) * kn[1];
+                        }
+                    }
+                }
+            }
+
+            // CPML on E, ref :6522-6670: Ex (y then z), Ey (x then z), Ez (x then y)
+            const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
+            const int q1l = ax1 == 0 ? qxl : qyl, q1h = ax1 == 0 ? qxh : qyh;
+            const int q2l = ax2 == 1 ? qyl : qzl, q2h = ax2 == 1 ? qyh : qzh;
+            const T t1 = comp == 2 ? d1 : (comp == 0 ? d1 : d1);  // difference along ax1
+            const T t2 = d2;                                     // difference along ax2
+            if (q1l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][0], P.be[ax1][0][q1l - 1], P.ce[ax1][0][q1l - 1], t1, P.del[ax1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
+            if (q1h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][1], P.be[ax1][1][q1h - 1], P.ce[ax1][1][q1h - 1], t1, P.del[ax1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
+            if (q2l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][0], P.be[ax2][0][q2l - 1], P.ce[ax2][0][q2l - 1], t2, P.del[ax2], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
+            if (q2h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][1], P.be[ax2][1][q2h - 1], P.ce[ax2][1][q2h - 1], t2, P.del[ax2], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
+            st<T>(Ec, c, e);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+void launch_update_h(const AemParams& P, int counter, cudaStream_t s) {
+    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
+    if (P.kmax) k_update_h<cf><<<grd, blk, 0, s>>>(P, counter);
+    else k_update_h<float><<<grd, blk, 0, s>>>(P, counter);
+}
+void launch_update_e(const AemParams& P, int counter, cudaStream_t s) {
+    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
+    if (P.kmax) k_update_e<cf><<<grd, blk, 0, s>>>(P, counter);
+    else k_update_e<float><<<grd, blk, 0, s>>>(P, counter);
+}
+
+}  // namespace aem

@@ -1,0 +1,76 @@
+// aem_kernels.h -- launch interface of the per-step kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "aem_types.h"
+
+namespace aem {
+
+// one lumped port on the device (ref ports(:,:,:), Voltage/Current lines)
+struct PortDev {
+    int gridded, dir, side;
+    int loc[3], size[3];        // reference indices / cell counts (ports(i,3..4,:))
+    float sizef[3];             // ports(i,4,:) as reals
+    int n1, n2;                 // gridded feed extent
+    const float* feed;          // (4, n1+1, n2+1) F-order; gridded only
+    float feed_norm;            // mode normalisation (ref :4948-4954), host computed
+    float cI, cV, cS;           // (1/L)(dt/d), (1/C)(dt/d), (1/sqrt(CL))(dt/d)
+    float dl[3];                // del_x, del_y, del_z
+    void* V;                    // Voltage(1..P), complex when kmax
+    void* I;                    // Current(1..P-1)
+    void* vout;                 // Voltage_out(1..steps)
+    int excite;                 // this port is the excitation port
+};
+
+struct PortSet {
+    int n, P;                   // number of ports, port_array_size
+    PortDev p[AEM_MAX_PORTS];
+    const void* srcI;           // E_or_V_1D(amp, n, 0) per step (index n-1)
+    const void* srcV;           // E_or_V_1D(amp, n+0.5, 0.5 d) per step
+};
+
+// far-field Huygens box
+struct FarFieldDev {
+    int nang, len;              // angles, bins per series (len_ff + 2)
+    int lo[3], hi[3];           // ff_xlow.. (reference indices)
+    int has[3];                 // faces present per axis (non-periodic)
+    int ic, jc, kc;
+    float r_relay, c_dt;        // r_for_time_relay, c*dt
+    float fac[3];               // area/(4 pi dt c) per face normal
+    float wall_lo[3], wall_hi[3];
+    const float* ang;           // per angle: sin(th), cos(th), sin(ph), cos(ph)
+    void* cur[3][2];            // per face normal / side: 8 arrays (4 new + 4 old) contiguous
+    long long face_n[3];        // cells per face of that normal
+    void* UW;                   // [6][nang][len]: Wx,Wy,Wz,Ux,Uy,Uz
+    int mirror;                 // image-ground-plane pass
+    float mir_off[3], use_mir[3], M_mir[3], J_mir[3];
+    float kc3[3];               // kmax: k_count for Bloch-phase removal
+};
+
+// per-step output taps
+struct TapDev {
+    int plane_sum;              // standard unit-cell plane sums
+    int axis;                   // normal of the reflection/transmission planes
+    float w1, w2;               // projection weights (see plane_sum kernel)
+    void* refl;                 // per step
+    void* trans;
+    void* refl_tm;              // kmax: TM sums (refl/trans above are TE)
+    void* trans_tm;
+    float knum[3];
+    int ff_pc;                  // phase-centre sample
+    int ic, jc, kc;
+    void* pc[6];                // Ex,Ey,Ez,Hx,Hy,Hz per step (+1)
+    int video;                  // 2-D slice export
+    int slice_dir, slice_loc, v1, v2;
+    void* vid[6];               // Ex,Hx,Ey,Hy,Ez,Hz each (v1, v2, steps)
+};
+
+void launch_update_h(const AemParams& P, int counter, cudaStream_t s);
+void launch_update_e(const AemParams& P, int counter, cudaStream_t s);
+void launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
+void launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
+void launch_ff_currents(const AemParams& P, const FarFieldDev& F, cudaStream_t s);
+void launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s);
+void launch_taps(const AemParams& P, const TapDev& T, const FarFieldDev& F, int counter, int steps, cudaStream_t s);
+
+}  // namespace aem

@@ -1,0 +1,64 @@
+// aem_model.h -- host-side model built from a Deck: the data that is
+// uploaded once to the GPU before the time loop.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "aem_deck.h"
+#include "aem_types.h"
+
+namespace aem {
+
+struct SheetPlaneHost {
+    int axis = 0, pos = 0;        // normal axis, reference index along it
+    int na = 0, nb = 0, pa = 0;   // in-plane storage extents and pitch
+    std::vector<uint8_t> nmask, tmask;
+    std::vector<float> sa, sb, ga1, gb1, ga2, gb2;
+};
+
+struct HostModel {
+    Deck d;
+    int S[3] = {0, 0, 0};   // storage extents per axis
+    int PX = 0;             // x pitch
+    long long plane = 0, cells = 0;
+    std::vector<uint8_t> cell_id;                 // [SZ][SY][PX], 0 = vacuum
+    std::vector<AemMaterial> mats;                // 0 = vacuum, 1.. = deck volume materials
+    std::vector<AemUniformCoef> ucoef;            // same indexing
+    int npoles = 0;
+    bool has_drude = false;
+    int dbox[3][6] = {};                          // Drude boxes (reference indices)
+    std::vector<SheetPlaneHost> splanes;
+    std::vector<float> den_e[3], den_h[3];        // index 0..N-1 holds den(1..N-1) at [idx-1]
+    float be[3][2][AEM_MAX_PML] = {}, ce[3][2][AEM_MAX_PML] = {};
+    float bh[3][2][AEM_MAX_PML] = {}, ch[3][2][AEM_MAX_PML] = {};
+    std::vector<std::vector<float>> feeds;        // per port: gridded feed (4, n1+1, n2+1), F-order
+    int feed_m1 = 0, feed_m2 = 0;                 // reference array extents (max n1+1, max n2+1)
+    std::vector<float> geometry;                  // (4, gx, gy, gz) F-order float32 for _geometry.bin
+
+    // storage position of reference index `idx` on axis a (wraps when periodic)
+    int pos(int a, int idx) const {
+        if (d.pbc[a]) {
+            int n = S[a];
+            int p = (idx - 1) % n;
+            return p < 0 ? p + n : p;
+        }
+        return idx - 1;
+    }
+    long long lin(int i, int j, int k) const {  // reference cell/edge indices
+        return ((long long)pos(2, k) * S[1] + pos(1, j)) * PX + pos(0, i);
+    }
+};
+
+// Build the model: geometry rasterisation, material tables, sheets, Drude
+// boxes, CPML tables and gridded feeds.  `workdir` resolves relative file
+// names (bulk geometry, gridded feeds).  Throws DeckError.
+void build_model(HostModel& m, const std::string& workdir);
+
+// Edge coefficients as the reference computes them from the averaged cell
+// properties (used by the host for sheet overrides and by tests).
+void edge_material(const HostModel& m, int comp, int i, int j, int k, float* eps, float* sig,
+                   float* wp /*[npoles]*/, float* gam /*[npoles]*/);
+
+}  // namespace aem

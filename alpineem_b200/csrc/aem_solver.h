@@ -1,0 +1,77 @@
+// aem_solver.h -- one FDTD run on one GPU: the device state of a deck and
+// the per-step launch sequence.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "aem_kernels.h"
+#include "aem_model.h"
+
+namespace aem {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+class Solver {
+   public:
+    // Parse `inputs_path` (relative files resolve against its directory),
+    // build the model and upload it to the current CUDA device.
+    Solver(const std::string& inputs_path, bool kmax, const std::string& outdir);
+    ~Solver();
+    Solver(const Solver&) = delete;
+    Solver& operator=(const Solver&) = delete;
+
+    // advance `n` time steps (bounded by the deck's step count)
+    void run(int n);
+    // post-loop processing and the reference output files (.dat, video)
+    void finalize_and_write();
+    // host copy of a final field component in the reference layout
+    // (comp 0..5 = Ex,Ey,Ez,Hx,Hy,Hz; real part and imaginary part (kmax))
+    void get_field(int comp, std::vector<double>& re, std::vector<double>& im, int dims[3]);
+
+    const Deck& deck() const { return m_.d; }
+    const std::vector<float>& geometry() const { return m_.geometry; }
+    int steps_done() const { return done_; }
+    size_t device_bytes() const { return dev_bytes_; }
+    cudaStream_t stream() const { return stream_; }
+    // bytes the fused Yee/CPML update must move per step (algorithmic)
+    double algorithmic_bytes_per_step() const;
+    long long cell_count() const;
+
+    // time series gathered on the host by finalize
+    std::vector<double> incident_re, incident_im;
+    std::vector<std::vector<double>> vout_re, vout_im;             // per port
+    std::vector<double> refl_re, refl_im, trans_re, trans_im;      // plane sums (TE for kmax)
+    std::vector<double> refl_tm_re, refl_tm_im, trans_tm_re, trans_tm_im;
+    std::vector<std::vector<double>> eth_re, eth_im, eph_re, eph_im;  // far field, per angle
+    std::vector<int> data_out_time;
+    std::vector<double> pc_re[3], pc_im[3];
+
+   private:
+    void* alloc(size_t bytes);
+    template <typename V>
+    void* upload(const std::vector<V>& v);
+    void setup_params();
+    void setup_ports();
+    void setup_farfield();
+    void setup_taps();
+    void step(int counter);
+
+    std::string outdir_;
+    HostModel m_;
+    AemParams P_{};
+    PortSet PS_{};
+    FarFieldDev FF_{};
+    TapDev TP_{};
+    std::vector<void*> bufs_;
+    size_t dev_bytes_ = 0;
+    int es_ = 4;  // bytes per field value
+    int done_ = 0;
+    cudaStream_t stream_ = nullptr;
+};
+
+}  // namespace aem

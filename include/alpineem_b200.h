@@ -1,0 +1,100 @@
+/*
+ * alpineem_b200.h -- C ABI of the B200 FDTD solver library
+ * (libalpineem_b200.so).
+ *
+ * The reference (DanRich123/AlpineEM) exposes its FDTD core as one
+ * executable: master.py writes a positional input deck and runs
+ * `./<solver> inputs.txt` (main_fdtd/master.py:438-441); the solver reads the
+ * deck named by argv[1] (main_fdtd/fdtd_solver.f90:726-727), runs the time
+ * loop (:4440-8299) and writes <name>.dat, <name>_geometry.bin and optional
+ * <name>_video_*.bin next to the deck (:2355-2357, :8538-8807), which
+ * utility_scripts/post_processor.py parses.  These entry points split that
+ * executable into create / run / write so a caller (the FDTD-B200 launcher,
+ * Python through ctypes) can drive it step by step.  Plain C types only.
+ *
+ * Errors: every function returns 0 on success and a negative AEM_ERR_* code
+ * otherwise; aem_last_error() returns the message (for invalid decks, the
+ * reference's own "ERROR: ..." text).  A handle is not thread-safe; distinct
+ * handles are independent.  Device memory belongs to the handle and is freed
+ * by aem_destroy.
+ */
+#ifndef ALPINEEM_B200_H
+#define ALPINEEM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct aem_handle aem_handle;
+
+#define AEM_OK 0
+#define AEM_ERR_INPUT (-1)    /* invalid deck or missing side file (reference STOP "ERROR: ...") */
+#define AEM_ERR_CUDA (-2)     /* CUDA runtime failure (no device, out of memory, launch error) */
+#define AEM_ERR_ARG (-3)      /* bad argument to this API */
+#define AEM_ERR_STATE (-4)    /* call out of order (e.g. write before the last step) */
+
+/* Deck grammar selector: the reference builds two solvers from one source
+ * (fdtd_solver.f90:5-7); AEM_KMAX selects the constant-k periodic one. */
+#define AEM_STANDARD 0
+#define AEM_KMAX 1
+
+/* Library version, encoded as major*10000 + minor*100 + patch. */
+int aem_version(void);
+
+/* Replaces the solver executable's start-up (fdtd_solver.f90:726-4355):
+ * parse the deck at `inputs_path` (side files resolve against its
+ * directory), build the model and upload it to the current CUDA device.
+ * Output files go to `outdir` (NULL: the current directory, like the
+ * reference).  Writes <name>_geometry.bin as the reference does. */
+int aem_create_from_file(const char* inputs_path, int mode, const char* outdir, aem_handle** out);
+
+/* Advance `nsteps` time steps of the reference loop (fdtd_solver.f90:4440,
+ * one `counter` per step), never past the deck's step count. */
+int aem_run(aem_handle* h, int nsteps);
+
+/* Steps done so far and the deck's step count. */
+int aem_steps(aem_handle* h, int* done, int* total);
+
+/* Wait for the device work queued on the handle's stream. */
+int aem_synchronize(aem_handle* h);
+
+/* Post-loop processing and the reference's output files
+ * (fdtd_solver.f90:8338-8807): <name>.dat and, when requested by the deck,
+ * <name>_video_*.bin.  Requires all steps to be done. */
+int aem_write_outputs(aem_handle* h);
+
+/* Time series after aem_write_outputs, as the .dat file holds them:
+ *   kind 0 incident, 1 reflected, 2 transmitted (TE for kmax),
+ *   3 reflected TM, 4 transmitted TM (kmax), 5 port voltage (index = port
+ *   0..), 6 far-field E_theta (index = angle), 7 far-field E_phi.
+ * Copies min(n, steps) values; im may be NULL. */
+int aem_get_series(aem_handle* h, int kind, int index, double* re, double* im, int n);
+
+/* Final field component in the reference's array layout (first index
+ * fastest): comp 0..5 = Ex, Ey, Ez, Hx, Hy, Hz with the extents of
+ * fdtd_solver.f90:3908-3913.  `dims` receives the extents; re/im must hold
+ * dims[0]*dims[1]*dims[2] values (pass NULL first to query dims).  im may be
+ * NULL. */
+int aem_get_field(aem_handle* h, int comp, int dims[3], double* re, double* im);
+
+/* Reference grid sizes X, Y, Z (cells per axis + 1 + periodic layer,
+ * fdtd_solver.f90:1316-1318). */
+int aem_grid(aem_handle* h, int sizes[3]);
+
+/* Bytes of device memory held by the handle. */
+int aem_device_bytes(aem_handle* h, size_t* bytes);
+
+/* Message of the last failing call on this handle (or of the last failing
+ * aem_create_* when h is NULL).  Valid until the next call. */
+const char* aem_last_error(aem_handle* h);
+
+/* Free the handle and its device memory. */
+int aem_destroy(aem_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALPINEEM_B200_H */
