@@ -158,7 +158,8 @@ def csv_complex(path):
 
 def match_rows(freq_ref, freq, cols):
     """Pick the rows of (freq, cols) at the reference's (possibly thinned) frequencies."""
-    idx = np.searchsorted(freq, freq_ref - 1e-9)
-    idx = np.clip(idx, 0, len(freq) - 1)
-    assert np.max(np.abs(freq[idx] - freq_ref)) < 1e-6, "frequency grids differ"
+    idx = np.clip(np.searchsorted(freq, freq_ref), 1, len(freq) - 1)
+    idx = np.where(np.abs(freq[idx - 1] - freq_ref) < np.abs(freq[idx] - freq_ref), idx - 1, idx)
+    # the .dat holds dt to 10 significant digits, so the grids agree to ~1e-8 relative
+    assert np.max(np.abs(freq[idx] - freq_ref) / np.maximum(np.abs(freq_ref), 1e-3)) < 1e-6, "frequency grids differ"
     return [c[idx] for c in cols]
