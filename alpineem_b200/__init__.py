@@ -60,8 +60,34 @@ def load_library():
     lib.aem_last_error.argtypes = [h]
     lib.aem_last_error.restype = ctypes.c_char_p
     lib.aem_destroy.argtypes = [h]
+    lib.aem_create_from_memory.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(h)]
+    lib.aem_check_deck.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.aem_read_probe.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.aem_profile.argtypes = [h, ctypes.c_int]
+    lib.aem_profile_read.argtypes = [h, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+    lib.aem_launch_count.argtypes = [h, ctypes.POINTER(ctypes.c_longlong)]
+    lib.aem_workload.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
+    lib.aem_flush.argtypes = [h]
+    lib.aem_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]
+    lib.aem_transfer_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     _lib = lib
     return lib
+
+
+PHASES = ["update_h", "update_e", "ports", "ff_currents", "ff_bin", "taps", "yee", "other"]
+
+
+def check_deck(deck_text, ext_text=None, kmax=False):
+    """Validate a deck without a GPU; returns the reference grid sizes
+    (X, Y, Z) or raises AemError with the reference's "ERROR: ..." text."""
+    lib = load_library()
+    g = (ctypes.c_int * 3)()
+    rc = lib.aem_check_deck(deck_text.encode(), ext_text.encode() if ext_text else None, KMAX if kmax else STANDARD, g)
+    if rc != 0:
+        raise AemError(lib.aem_last_error(None).decode())
+    return tuple(g)
 
 
 def _dptr(a):
@@ -78,11 +104,21 @@ class Simulation:
     directory, like the reference executable).
     """
 
-    def __init__(self, inputs_path, kmax=False, outdir=None):
+    def __init__(self, inputs_path=None, kmax=False, outdir=None, deck_text=None, ext_text=None, bulk=None):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
-        rc = self._lib.aem_create_from_file(os.fsencode(inputs_path), KMAX if kmax else STANDARD,
-                                            os.fsencode(outdir) if outdir else None, ctypes.byref(self._h))
+        mode = KMAX if kmax else STANDARD
+        od = os.fsencode(outdir) if outdir else None
+        if deck_text is None:
+            rc = self._lib.aem_create_from_file(os.fsencode(inputs_path), mode, od, ctypes.byref(self._h))
+        else:
+            ptr, n = None, 0
+            if bulk is not None:
+                if bulk.dtype != np.float32 or not bulk.flags.c_contiguous:
+                    raise ValueError("bulk must be a contiguous float32 array (x fastest)")
+                ptr, n = bulk.ctypes.data, bulk.size
+            rc = self._lib.aem_create_from_memory(deck_text.encode(), ext_text.encode() if ext_text else None, ptr, n,
+                                                  mode, od, ctypes.byref(self._h))
         if rc != 0:
             raise AemError(self._lib.aem_last_error(None).decode())
         self.kmax = kmax
@@ -146,6 +182,58 @@ class Simulation:
         shape = (dims[2], dims[1], dims[0])
         out = re.reshape(shape)
         return out + 1j * im.reshape(shape) if self.kmax else out
+
+    def probe(self, kind, index=0, first=1, n=None):
+        """Raw per-step samples of the steps run so far (port voltage or
+        unnormalised plane sums); synchronises."""
+        k = SERIES[kind] if isinstance(kind, str) else int(kind)
+        if n is None:
+            n = self.steps[0] - first + 1
+        re, im = np.zeros(n), np.zeros(n)
+        self._check(self._lib.aem_read_probe(self._h, k, int(index), int(first), int(n), _dptr(re), _dptr(im)))
+        return (re + 1j * im) if self.kmax else re
+
+    def profile(self, enable=True):
+        """Turn per-phase event timing on (clearing the record) or off."""
+        self._check(self._lib.aem_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{phase: (milliseconds, launches)} since profiling was turned on."""
+        ms = (ctypes.c_double * len(PHASES))()
+        nl = (ctypes.c_longlong * len(PHASES))()
+        self._check(self._lib.aem_profile_read(self._h, ms, nl))
+        return {PHASES[p]: (ms[p], nl[p]) for p in range(len(PHASES))}
+
+    def flush(self):
+        """Bin the far-field contributions still held in the 32-step batch buffer."""
+        self._check(self._lib.aem_flush(self._h))
+
+    @property
+    def stream(self):
+        """The cudaStream_t the solver launches on (an integer handle)."""
+        s = ctypes.c_void_p()
+        self._check(self._lib.aem_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    @property
+    def transfer_bytes(self):
+        """(host->device, device->host) bytes copied so far."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self._lib.aem_transfer_bytes(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    @property
+    def launches(self):
+        n = ctypes.c_longlong()
+        self._check(self._lib.aem_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    @property
+    def workload(self):
+        """(cells per step as the reference counts them, algorithmic bytes per step)."""
+        c, b = ctypes.c_longlong(), ctypes.c_double()
+        self._check(self._lib.aem_workload(self._h, ctypes.byref(c), ctypes.byref(b)))
+        return c.value, b.value
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

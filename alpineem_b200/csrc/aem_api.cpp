@@ -31,6 +31,8 @@ int guarded(aem_handle* h, F&& f) {
         return f();
     } catch (const aem::DeckError& e) {
         return fail(h, AEM_ERR_INPUT, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(h, AEM_ERR_ARG, e.what());
     } catch (const std::runtime_error& e) {
         std::string m = e.what();
         return fail(h, m.rfind("CUDA", 0) == 0 ? AEM_ERR_CUDA : AEM_ERR_INPUT, m);
@@ -44,25 +46,66 @@ extern "C" {
 
 int aem_version(void) { return 1 * 10000 + 0 * 100 + 0; }
 
+// <name>_geometry.bin, ref :2355-2357 (skipped with the geometry_bin no extension)
+static void write_geometry(const aem::Solver& s, const std::string& od) {
+    const aem::Deck& d = s.deck();
+    if (!d.ext_geometry_bin) return;
+    std::string base = d.filename.substr(0, d.filename.size() >= 4 ? d.filename.size() - 4 : 0);
+    std::string fn = (od.empty() ? "" : od + "/") + base + "_geometry.bin";
+    FILE* f = std::fopen(fn.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write '" + fn + "'");
+    const std::vector<float>& g = s.geometry();
+    size_t w = std::fwrite(g.data(), sizeof(float), g.size(), f);
+    std::fclose(f);
+    if (w != g.size()) throw std::runtime_error("short write to '" + fn + "'");
+}
+
+static int need_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, AEM_ERR_CUDA, "CUDA error: no usable CUDA device");
+    }
+    return AEM_OK;
+}
+
 int aem_create_from_file(const char* inputs_path, int mode, const char* outdir, aem_handle** out) {
     if (!inputs_path || !out || (mode != AEM_STANDARD && mode != AEM_KMAX)) return fail(nullptr, AEM_ERR_ARG, "bad argument");
     *out = nullptr;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, AEM_ERR_CUDA, "CUDA error: no usable CUDA device");
+    if (int rc = need_device()) return rc;
     return guarded(nullptr, [&]() {
         auto h = std::make_unique<aem_handle>();
         std::string od = outdir ? outdir : "";
         h->s = std::make_unique<aem::Solver>(inputs_path, mode == AEM_KMAX, od);
-        // <name>_geometry.bin, ref :2355-2357
-        const aem::Deck& d = h->s->deck();
-        std::string base = d.filename.substr(0, d.filename.size() >= 4 ? d.filename.size() - 4 : 0);
-        std::string fn = (od.empty() ? "" : od + "/") + base + "_geometry.bin";
-        if (FILE* f = std::fopen(fn.c_str(), "wb")) {
-            const std::vector<float>& g = h->s->geometry();
-            std::fwrite(g.data(), sizeof(float), g.size(), f);
-            std::fclose(f);
-        }
+        write_geometry(*h->s, od);
         *out = h.release();
+        return AEM_OK;
+    });
+}
+
+int aem_create_from_memory(const char* deck_text, const char* ext_text, const float* bulk, size_t bulk_count, int mode,
+                           const char* outdir, aem_handle** out) {
+    if (!deck_text || !out || (mode != AEM_STANDARD && mode != AEM_KMAX) || (bulk_count && !bulk))
+        return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    *out = nullptr;
+    if (int rc = need_device()) return rc;
+    return guarded(nullptr, [&]() {
+        auto h = std::make_unique<aem_handle>();
+        std::string od = outdir ? outdir : "";
+        h->s = std::make_unique<aem::Solver>(deck_text, ext_text ? ext_text : "", bulk, bulk_count, mode == AEM_KMAX, od, od);
+        write_geometry(*h->s, od);
+        *out = h.release();
+        return AEM_OK;
+    });
+}
+
+int aem_check_deck(const char* deck_text, const char* ext_text, int mode, int sizes[3]) {
+    if (!deck_text || (mode != AEM_STANDARD && mode != AEM_KMAX)) return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    return guarded(nullptr, [&]() {
+        aem::Deck d = aem::parse_deck(deck_text, mode == AEM_KMAX);
+        aem::apply_extensions(d, ext_text ? ext_text : "");
+        aem::derive(d);
+        if (sizes) { sizes[0] = d.X; sizes[1] = d.Y; sizes[2] = d.Z; }
         return AEM_OK;
     });
 }
@@ -137,6 +180,64 @@ int aem_get_field(aem_handle* h, int comp, int dims[3], double* re, double* im) 
         if (im) std::memcpy(im, i.data(), sizeof(double) * i.size());
         return AEM_OK;
     });
+}
+
+int aem_profile(aem_handle* h, int enable) {
+    if (!h) return AEM_ERR_ARG;
+    return guarded(h, [&]() {
+        h->s->set_profiling(enable != 0);
+        return AEM_OK;
+    });
+}
+
+int aem_profile_read(aem_handle* h, double ms[AEM_NPHASE], long long launches[AEM_NPHASE]) {
+    if (!h || !ms || !launches) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->read_profile(ms, launches);
+        return AEM_OK;
+    });
+}
+
+int aem_flush(aem_handle* h) {
+    if (!h) return AEM_ERR_ARG;
+    return guarded(h, [&]() {
+        h->s->flush();
+        return AEM_OK;
+    });
+}
+
+int aem_stream(aem_handle* h, void** stream) {
+    if (!h || !stream) return fail(h, AEM_ERR_ARG, "bad argument");
+    *stream = (void*)h->s->stream();
+    return AEM_OK;
+}
+
+int aem_transfer_bytes(aem_handle* h, long long* h2d, long long* d2h) {
+    if (!h) return AEM_ERR_ARG;
+    if (h2d) *h2d = (long long)h->s->h2d_bytes();
+    if (d2h) *d2h = (long long)h->s->d2h_bytes();
+    return AEM_OK;
+}
+
+int aem_launch_count(aem_handle* h, long long* n) {
+    if (!h || !n) return fail(h, AEM_ERR_ARG, "bad argument");
+    *n = h->s->launches();
+    return AEM_OK;
+}
+
+int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, double* re, double* im) {
+    if (!h || !re || n < 0) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->read_probe(kind, index, first_step, n, re, im);
+        return AEM_OK;
+    });
+}
+
+int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step) {
+    if (!h) return AEM_ERR_ARG;
+    if (cells) *cells = h->s->cell_count();
+    if (bytes_per_step) *bytes_per_step = h->s->algorithmic_bytes_per_step();
+    return AEM_OK;
 }
 
 int aem_grid(aem_handle* h, int sizes[3]) {

@@ -194,7 +194,7 @@ __device__ inline cf unphase<cf>(const AemParams& P, const FarFieldDev& F, cf v,
 }
 
 template <typename T>
-__global__ void k_ff_currents(const __grid_constant__ AemParams P, const __grid_constant__ FarFieldDev F) {
+__global__ void k_ff_currents(const __grid_constant__ AemParams P, const __grid_constant__ FarFieldDev F, int slot) {
     const long long tot = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]);
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < tot; g += (long long)gridDim.x * blockDim.x) {
         long long r = g;
@@ -229,11 +229,13 @@ __global__ void k_ff_currents(const __grid_constant__ AemParams P, const __grid_
             v[2] = sg * ((fget<T>(P, Hy, i, j, k) + fget<T>(P, Hy, i, j + 1, k)) / 2.0f) * w;
             v[3] = (-1.0f * sg) * ((fget<T>(P, Hx, i, j, k) + fget<T>(P, Hx, i + 1, j, k)) / 2.0f) * w;
         }
-        T* base = reinterpret_cast<T*>(F.cur[a][s]);
+        T* cur = reinterpret_cast<T*>(F.cur[a][s]);
+        T* dif = reinterpret_cast<T*>(F.dbuf[a][s]);
         const long long n = F.face_n[a];
         for (int m = 0; m < 4; m++) {
-            base[(4 + m) * n + q] = base[m * n + q];
-            base[m * n + q] = unphase<T>(P, F, v[m], i, j, k, a);
+            const T nv = unphase<T>(P, F, v[m], i, j, k, a);
+            dif[((long long)m * F.tb + slot) * n + q] = nv - cur[m * n + q];  // M - M_o, ref :7667
+            cur[m * n + q] = nv;
         }
     }
 }
@@ -266,10 +268,10 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
         idx[a] = s ? F.hi[a] : F.lo[a];
         idx[b] = F.lo[b] + (int)(q % nb);
         idx[c] = F.lo[c] + (int)(q / nb);
-        const T* base = reinterpret_cast<const T*>(F.cur[a][s]);
+        const T* dif = reinterpret_cast<const T*>(F.dbuf[a][s]);
         const long long n = F.face_n[a];
         T d[4];
-        for (int m = 0; m < 4; m++) d[m] = base[m * n + q] - base[(4 + m) * n + q];
+        for (int m = 0; m < 4; m++) d[m] = dif[(long long)m * F.tb * n + q];  // slot 0
         // component slots: W = 0..2, U = 3..5; (M1, M2, J1, J2) per face normal
         const int u1 = a == 0 ? 4 : 3, u2 = a == 2 ? 4 : 5, w1 = a == 0 ? 1 : 0, w2 = a == 2 ? 1 : 2;
         const float* A = F.ang + 4 * ang;  // sin(th), cos(th), sin(ph), cos(ph)
@@ -303,6 +305,137 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
             atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[3] * sm[3]));
             atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii], wt * fac * (d[3] * sm[3]));
         }
+    }
+}
+
+// Time-batched retarded-time binning (FP32 fields).  The contribution of face
+// cell c at step n to angle g is the reference's (ref :7667-7730)
+//   t = n + 1/2 + tf(c,g) - 1 (U, from M)   or   n + tf(c,g) - 1 (W, from J),
+//   U(ii) += (1-w) fac dM,  U(ii+1) += w fac dM,  ii = int(t), w = t - ii,
+// with tf(c,g) fixed over the run.  The differences of F.tb steps are kept
+// (F.dbuf) and binned here in one pass: a CTA takes one 32x32 tile of one face
+// and F.group virtual angles (angle, image pass); lane t of each warp owns
+// step n0+t and holds the differences of 16 cells of one tile row in
+// registers.  For every angle the lane walks its 16 cells, summing the two
+// interpolation weights in registers while the bin stays the same and adding
+// the sums into a shared histogram when it changes (lanes own distinct bins,
+// so the shared atomics never collide within an instruction).  Each histogram
+// goes to U/W once per batch, one global atomic per non-zero bin, scaled by
+// fac and the image-pass sign.  tf(c,g) = K0 + Ku*u + Kv*v over the face's
+// (u, v) cell indices (host-precomputed per angle and face).
+__global__ void __launch_bounds__(256, 1) k_ff_bin_batch(const __grid_constant__ AemParams P,
+                                                         const __grid_constant__ FarFieldDev F, int n0, int nt) {
+    extern __shared__ float hist[];  // [group][4][hspan]: U1, U2, W1, W2
+    __shared__ float ksh[64][3];
+    __shared__ int bsh[64];
+    const int G = F.group, HS = F.hspan;
+    // face (a, s) of this tile
+    const long long tile = blockIdx.x;
+    int f = 0;
+    while (f < 5 && tile >= F.tile0[f + 1]) f++;
+    const int a = f >> 1, s = f & 1;
+    const long long tl = tile - F.tile0[f];
+    const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+    const int nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
+    const int u0 = (int)(tl % F.tiles_u[a]) * FF_TILE, v0 = (int)(tl / F.tiles_u[a]) * FF_TILE;
+    const int va0 = blockIdx.y * G;
+    const int ng = min(G, F.nvang - va0);
+    const long long n = F.face_n[a];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    for (int e = tid; e < G * 4 * HS; e += blockDim.x) hist[e] = 0.0f;
+    if (tid < ng) {
+        const float* k = F.kf + (((long long)(va0 + tid) * 3 + a) * 2 + s) * 3;
+        ksh[tid][0] = k[0]; ksh[tid][1] = k[1]; ksh[tid][2] = k[2];
+        // lowest bin any contribution of the tile can reach, less a margin
+        const float tmin = k[0] + k[1] * (float)(k[1] < 0.0f ? u0 + FF_TILE - 1 : u0) +
+                           k[2] * (float)(k[2] < 0.0f ? v0 + FF_TILE - 1 : v0);
+        bsh[tid] = (int)floorf((float)n0 + tmin - 1.0f) - 3;
+    }
+    __syncthreads();
+
+    const float fn = (float)(n0 + lane), fnh = fn + 0.5f;
+    const bool live = lane < nt;
+    const float* dif = reinterpret_cast<const float*>(F.dbuf[a][s]);
+    int bad = 0;
+    for (int sub = 0; sub < FF_TILE / 4; sub++) {
+        const int v = v0 + 4 * sub + (warp >> 1);
+        const int ub0 = u0 + 16 * (warp & 1);
+        if (v >= nc || ub0 >= nb) continue;  // warp-uniform
+        float d[16][4];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const bool ok = live && ub0 + j < nb;
+            const long long q = (long long)v * nb + ub0 + j;
+#pragma unroll
+            for (int m = 0; m < 4; m++) d[j][m] = ok ? __ldg(dif + ((long long)m * F.tb + lane) * n + q) : 0.0f;
+        }
+        for (int g = 0; g < ng; g++) {
+            const float tf0 = fmaf(ksh[g][2], (float)v, ksh[g][0]), ku = ksh[g][1];
+            // histogram offsets: bin k of component m of angle g is hist[(4g+m)HS + k - bsh[g]]
+            const int oU1 = g * 4 * HS - bsh[g], oU2 = oU1 + HS, oW1 = oU1 + 2 * HS, oW2 = oU1 + 3 * HS;
+            int kU = INT_MIN, kW = INT_MIN;
+            float u1l = 0.0f, u1h = 0.0f, u2l = 0.0f, u2h = 0.0f, w1l = 0.0f, w1h = 0.0f, w2l = 0.0f, w2h = 0.0f;
+            const int lo_ok = bsh[g], hi_ok = bsh[g] + HS - 1;
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const float tf = fmaf(ku, (float)(ub0 + j), tf0);
+                const float tu = (fnh + tf) - 1.0f;
+                const int iu = (int)tu;
+                const float wu = tu - (float)iu;
+                const float tw = (fn + tf) - 1.0f;
+                const int iw = (int)tw;
+                const float ww = tw - (float)iw;
+                if (iu != kU) {
+                    if (kU != INT_MIN) {
+                        if (kU - 1 >= lo_ok && kU <= hi_ok) {
+                            atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
+                            atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
+                        } else bad++;
+                    }
+                    kU = iu; u1l = u1h = u2l = u2h = 0.0f;
+                }
+                if (iw != kW) {
+                    if (kW != INT_MIN) {
+                        if (kW - 1 >= lo_ok && kW <= hi_ok) {
+                            atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
+                            atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
+                        } else bad++;
+                    }
+                    kW = iw; w1l = w1h = w2l = w2h = 0.0f;
+                }
+                u1l = fmaf(1.0f - wu, d[j][0], u1l); u1h = fmaf(wu, d[j][0], u1h);
+                u2l = fmaf(1.0f - wu, d[j][1], u2l); u2h = fmaf(wu, d[j][1], u2h);
+                w1l = fmaf(1.0f - ww, d[j][2], w1l); w1h = fmaf(ww, d[j][2], w1h);
+                w2l = fmaf(1.0f - ww, d[j][3], w2l); w2h = fmaf(ww, d[j][3], w2h);
+            }
+            if (kU - 1 >= lo_ok && kU <= hi_ok) {
+                atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
+                atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
+            } else bad++;
+            if (kW - 1 >= lo_ok && kW <= hi_ok) {
+                atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
+                atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
+            } else bad++;
+        }
+    }
+    if (bad) atomicAdd(F.err, bad);
+    __syncthreads();
+
+    // histogram -> U/W; component slots (W = 0..2, U = 3..5) of (M1, M2, J1, J2)
+    const int mc1 = b, mc2 = c;  // tangential axes
+    float* UW = reinterpret_cast<float*>(F.UW);
+    for (int e = tid; e < ng * 4 * HS; e += blockDim.x) {
+        const float h = hist[e];
+        if (h == 0.0f) continue;
+        const int g = e / (4 * HS), m = (e / HS) & 3, k = e % HS;
+        const int va = va0 + g, ang = va % F.nang, pass = va / F.nang;
+        const long long gi = (long long)bsh[g] + k;
+        if (gi < 0 || gi >= F.len) { atomicAdd(F.err, 1); continue; }
+        float sg = 1.0f;
+        if (pass) sg = m == 0 ? F.M_mir[mc1] : m == 1 ? F.M_mir[mc2] : m == 2 ? F.J_mir[mc1] : F.J_mir[mc2];
+        const int slotc = m == 0 ? (a == 0 ? 4 : 3) : m == 1 ? (a == 2 ? 4 : 5) : m == 2 ? (a == 0 ? 1 : 0) : (a == 2 ? 1 : 2);
+        atomicAdd(&UW[((long long)slotc * F.nang + ang) * F.len + gi], h * F.fac[a] * sg);
     }
 }
 
@@ -398,40 +531,61 @@ __global__ void k_video(const __grid_constant__ AemParams P, const __grid_consta
 }
 
 // ---------------------------------------------------------------------------
-void launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s) {
-    if (!ps.n) return;
+int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s) {
+    if (!ps.n) return 0;
     if (P.kmax) k_ports_h<cf><<<1, 512, 0, s>>>(P, ps, counter);
     else k_ports_h<float><<<1, 512, 0, s>>>(P, ps, counter);
+    return 1;
 }
-void launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s) {
-    if (!ps.n) return;
+int launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s) {
+    if (!ps.n) return 0;
     if (P.kmax) k_ports_e<cf><<<1, 512, 0, s>>>(P, ps, counter);
     else k_ports_e<float><<<1, 512, 0, s>>>(P, ps, counter);
+    return 1;
 }
-void launch_ff_currents(const AemParams& P, const FarFieldDev& F, cudaStream_t s) {
-    if (!F.nang) return;
+int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaStream_t s) {
+    if (!F.nang) return 0;
     long long tot = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]);
+    if (tot == 0) return 0;
     int blocks = (int)((tot + 255) / 256 < 148 * 16 ? (tot + 255) / 256 : 148 * 16);
-    if (P.kmax) k_ff_currents<cf><<<blocks, 256, 0, s>>>(P, F);
-    else k_ff_currents<float><<<blocks, 256, 0, s>>>(P, F);
+    if (P.kmax) k_ff_currents<cf><<<blocks, 256, 0, s>>>(P, F, slot);
+    else k_ff_currents<float><<<blocks, 256, 0, s>>>(P, F, slot);
+    return 1;
 }
-void launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s) {
-    if (!F.nang) return;
+int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s) {
+    if (!F.nang) return 0;
     long long tot = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]) * F.nang;
+    if (tot == 0) return 0;
     int blocks = (int)((tot + 255) / 256 < 148 * 32 ? (tot + 255) / 256 : 148 * 32);
     if (P.kmax) k_ff_bin<cf><<<blocks, 256, 0, s>>>(P, F, counter);
     else k_ff_bin<float><<<blocks, 256, 0, s>>>(P, F, counter);
+    return 1;
 }
-void launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {
+size_t ff_batch_smem(const FarFieldDev& F) { return (size_t)F.group * 4 * F.hspan * sizeof(float); }
+int launch_ff_bin_batch(const AemParams& P, const FarFieldDev& F, int n0, int nt, cudaStream_t s) {
+    if (!F.nang || nt <= 0 || F.tile0[6] == 0) return 0;
+    dim3 grid((unsigned)F.tile0[6], (unsigned)((F.nvang + F.group - 1) / F.group));
+    k_ff_bin_batch<<<grid, 256, ff_batch_smem(F), s>>>(P, F, n0, nt);
+    return 1;
+}
+void ff_batch_prepare() {
+    // the histograms may exceed the 48 KB default of dynamic shared memory
+    cudaFuncSetAttribute(k_ff_bin_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+int launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {
+    int n = 0;
     if (D.plane_sum || D.ff_pc) {
         if (P.kmax) k_taps<cf><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
         else k_taps<float><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
+        n++;
     }
     if (D.video) {
-        int n = D.v1 * D.v2;
-        if (P.kmax) k_video<cf><<<(n + 255) / 256, 256, 0, s>>>(P, D, counter, steps);
-        else k_video<float><<<(n + 255) / 256, 256, 0, s>>>(P, D, counter, steps);
+        int cells = D.v1 * D.v2;
+        if (P.kmax) k_video<cf><<<(cells + 255) / 256, 256, 0, s>>>(P, D, counter, steps);
+        else k_video<float><<<(cells + 255) / 256, 256, 0, s>>>(P, D, counter, steps);
+        n++;
     }
+    return n;
 }
 
 }  // namespace aem

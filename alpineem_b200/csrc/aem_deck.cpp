@@ -7,6 +7,7 @@
 // reference's operation order, so the coefficients fed to the kernels equal
 // the reference's.
 #include "aem_deck.h"
+#include "aem_types.h"
 
 #include <cmath>
 #include <cstdio>
@@ -306,15 +307,35 @@ Deck parse_deck_file(const std::string& path, bool kmax) {
     ss << f.rdbuf();
     Deck d = parse_deck(ss.str(), kmax);
     // optional sidecar with run extensions
-    std::ifstream x(path + ".b200");
+    std::ifstream x(path + ".b200", std::ios::binary);
     if (x) {
-        std::string key;
-        while (x >> key) {
-            if (key == "pml_cells") x >> d.ext_pml_cells;
-            else { std::string rest; std::getline(x, rest); }
-        }
+        std::stringstream xs;
+        xs << x.rdbuf();
+        apply_extensions(d, xs.str());
     }
     return d;
+}
+
+void apply_extensions(Deck& d, const std::string& text) {
+    std::istringstream x(text);
+    std::string line;
+    while (std::getline(x, line)) {
+        std::istringstream ls(line);
+        std::string key, val;
+        if (!(ls >> key) || key[0] == '#') continue;
+        if (!(ls >> val)) throw DeckError("extension '" + key + "' needs a value");
+        if (key == "pml_cells") {
+            char* end = nullptr;
+            long v = std::strtol(val.c_str(), &end, 10);
+            if (*end || v < 0 || v > AEM_MAX_PML - 2) throw DeckError("extension pml_cells must be 0.." + std::to_string(AEM_MAX_PML - 2));
+            d.ext_pml_cells = (int)v;
+        } else if (key == "geometry_bin") {
+            if (val != "yes" && val != "no") throw DeckError("extension geometry_bin must be yes or no");
+            d.ext_geometry_bin = val == "yes";
+        } else {
+            throw DeckError("unknown extension '" + key + "'");
+        }
+    }
 }
 
 // ref :1305-1812 (FP32, same operation order as the reference)

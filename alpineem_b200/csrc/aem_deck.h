@@ -105,9 +105,12 @@ struct Deck {
     int k_pl_H = 0, k_pl_E = 0;
     float knum[3] = {};
 
-    // extension (sidecar "<inputs>.b200"): override the CPML thickness (in
-    // cells) and grading used by a run; 0 = reference default
+    // extensions (sidecar "<inputs>.b200", or the text passed to
+    // aem_create_from_memory), one "key value" per line:
+    //   pml_cells N      CPML thickness in cells (0 = reference default, 10)
+    //   geometry_bin no  do not build or write <name>_geometry.bin
     int ext_pml_cells = 0;
+    bool ext_geometry_bin = true;
 };
 
 // Parse an inputs.txt.  `kmax` selects the constant-k periodic grammar
@@ -115,6 +118,8 @@ struct Deck {
 // reference's "ERROR: ..." text on invalid input.
 Deck parse_deck(const std::string& text, bool kmax);
 Deck parse_deck_file(const std::string& path, bool kmax);
+// apply extension lines ("key value") to a parsed deck; unknown keys are errors
+void apply_extensions(Deck& d, const std::string& text);
 void derive(Deck& d);
 
 }  // namespace aem

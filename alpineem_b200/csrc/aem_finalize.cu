@@ -26,9 +26,10 @@ namespace {
 using cplx = std::complex<float>;
 
 // device buffer -> host, complex or real
-std::vector<cplx> fetch(const void* dev, size_t n, bool kmax, cudaStream_t s) {
+std::vector<cplx> fetch(const void* dev, size_t n, bool kmax, cudaStream_t s, size_t& counter) {
     std::vector<cplx> out(n);
     if (!n) return out;
+    counter += n * (kmax ? sizeof(cplx) : sizeof(float));
     if (kmax) {
         AEM_CUDA(cudaMemcpyAsync(out.data(), dev, n * sizeof(cplx), cudaMemcpyDeviceToHost, s));
         AEM_CUDA(cudaStreamSynchronize(s));
@@ -54,15 +55,22 @@ void Solver::finalize_and_write() {
     const Deck& d = m_.d;
     const bool K = d.kmax;
     const int T = d.steps;
+    flush_farfield(done_);
     AEM_CUDA(cudaStreamSynchronize(stream_));
     const float mu0 = 1.25663706E-6f, ep0 = 8.85418782E-12f, c0 = 299792458.0f, pi = 3.14159265358979323846f;
+    if (FF_.err) {
+        int err = 0;
+        AEM_CUDA(cudaMemcpy(&err, FF_.err, sizeof err, cudaMemcpyDeviceToHost));
+        d2h_bytes_ += sizeof err;
+        if (err) throw std::runtime_error("far-field binning: " + std::to_string(err) + " contributions outside their histogram");
+    }
 
     // plane sums, normalised per ref :8342-8361 / :8412-8435
     std::vector<cplx> refl, trans, refl_tm, trans_tm;
     if (TP_.plane_sum) {
-        refl = fetch(TP_.refl, T, K, stream_);
-        trans = fetch(TP_.trans, T, K, stream_);
-        if (K) { refl_tm = fetch(TP_.refl_tm, T, K, stream_); trans_tm = fetch(TP_.trans_tm, T, K, stream_); }
+        refl = fetch(TP_.refl, T, K, stream_, d2h_bytes_);
+        trans = fetch(TP_.trans, T, K, stream_, d2h_bytes_);
+        if (K) { refl_tm = fetch(TP_.refl_tm, T, K, stream_, d2h_bytes_); trans_tm = fetch(TP_.trans_tm, T, K, stream_, d2h_bytes_); }
         const int a = TP_.axis, b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
         const int N[3] = {d.X, d.Y, d.Z};
         // the reference multiplies the two transverse (size-2.0) factors in the
@@ -112,7 +120,7 @@ void Solver::finalize_and_write() {
     data_out_time.assign(nff, 1);
     if (nff > 0) {
         const size_t L = FF_.len;
-        std::vector<cplx> uw = fetch(FF_.UW, 6 * (size_t)nff * L, K, stream_);
+        std::vector<cplx> uw = fetch(FF_.UW, 6 * (size_t)nff * L, K, stream_, d2h_bytes_);
         const float eta = std::sqrt(mu0 / ep0);
         for (int i = 0; i < nff; i++) {
             const float a1 = d.ff_theta[i], a2 = d.ff_phi[i];
@@ -139,10 +147,10 @@ void Solver::finalize_and_write() {
         }
     }
     std::vector<std::vector<cplx>> vout(d.ports.size());
-    for (size_t q = 0; q < d.ports.size(); q++) vout[q] = fetch(PS_.p[q].vout, T, K, stream_);
+    for (size_t q = 0; q < d.ports.size(); q++) vout[q] = fetch(PS_.p[q].vout, T, K, stream_, d2h_bytes_);
     std::vector<cplx> pc[3];
     if (TP_.ff_pc)
-        for (int c = 0; c < 3; c++) pc[c] = fetch(TP_.pc[c], T, K, stream_);
+        for (int c = 0; c < 3; c++) pc[c] = fetch(TP_.pc[c], T, K, stream_, d2h_bytes_);
 
     // keep host copies for callers of the library
     auto split = [](const std::vector<cplx>& v, std::vector<double>& re, std::vector<double>& im) {
@@ -248,7 +256,7 @@ void Solver::finalize_and_write() {
         const char* nm[6] = {"Ex", "Hx", "Ey", "Hy", "Ez", "Hz"};
         const size_t n = (size_t)TP_.v1 * TP_.v2 * T;
         for (int q = 0; q < 6; q++) {
-            std::vector<cplx> v = fetch(TP_.vid[q], n, K, stream_);
+            std::vector<cplx> v = fetch(TP_.vid[q], n, K, stream_, d2h_bytes_);
             std::string base = d.filename.substr(0, d.filename.size() >= 4 ? d.filename.size() - 4 : 0);
             std::string fn = (outdir_.empty() ? "" : outdir_ + "/") + base + "_video_" + nm[q] + ".bin";
             FILE* vf = std::fopen(fn.c_str(), "wb");
@@ -272,7 +280,7 @@ void Solver::get_field(int comp, std::vector<double>& re, std::vector<double>& i
     const int X = d.X, Y = d.Y, Z = d.Z;
     static const int ext[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {0, -1, -1}, {-1, 0, -1}, {-1, -1, 0}};
     dims[0] = X + ext[comp][0]; dims[1] = Y + ext[comp][1]; dims[2] = Z + ext[comp][2];
-    std::vector<cplx> all = fetch(comp < 3 ? P_.E[comp] : P_.H[comp - 3], (size_t)m_.cells, d.kmax, stream_);
+    std::vector<cplx> all = fetch(comp < 3 ? P_.E[comp] : P_.H[comp - 3], (size_t)m_.cells, d.kmax, stream_, d2h_bytes_);
     size_t n = (size_t)dims[0] * dims[1] * dims[2];
     re.assign(n, 0.0); im.assign(n, 0.0);
     const int N[3] = {X, Y, Z};

@@ -89,10 +89,12 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
         const T ez_ip = ld_up<T>(P, Ez, lin(P, pxn, py, pz), wx, 0);
         const T ez_jp = ld_up<T>(P, Ez, lin(P, px, pyn, pz), wy, 1);
 
+        T hxv = ld<T>(Hx, c), hyv = ld<T>(Hy, c), hzv = ld<T>(Hz, c);
+        if (P.cpml_split != 2) {
         // bulk, ref :4448-4479 (DA = 1)
-        T hxv = ld<T>(Hx, c) + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
-        T hyv = ld<T>(Hy, c) + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
-        T hzv = ld<T>(Hz, c) + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
+        hxv = hxv + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
+        hyv = hyv + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
+        hzv = hzv + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
 
         // Smith-Maloney sheets, ref :4486-4554
         for (int s = 0; s < P.nsheet; s++) {
@@ -199,8 +201,9 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
             }
         }
 
+        }  // cpml_split != 2
         // CPML on H, ref :5227-5375: Hx (y then z), Hy (x then z), Hz (x then y)
-        {
+        if (P.cpml_split != 1) {
             const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0;
             const int qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
             if (qy_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
@@ -378,7 +381,9 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemPar
             float ga = co.ga, gb = co.gb;
             if (P.nsheet) sheet_override(P, comp, px, py, pz, &ga, &gb);
             const T eold = ld<T>(Ec, c);
-            T e = ga * eold + gb * curl;
+            T e = eold;
+            if (P.cpml_split != 2) {
+            e = ga * eold + gb * curl;
 
             // sheet sub-cell field of the normal component, ref :5714-5780
             for (int s = 0; s < P.nsheet; s++) {
@@ -462,7 +467,12 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemPar
                 }
             }
 
+            }  // cpml_split != 2
             // CPML on E, ref :6522-6670: Ex (y then z), Ey (x then z), Ez (x then y)
+            if (P.cpml_split == 1) {
+                st<T>(Ec, c, e);
+                continue;
+            }
             const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
             const int q1l = ax1 == 0 ? qxl : qyl, q1h = ax1 == 0 ? qxh : qyh;
             const int q2l = ax2 == 1 ? qyl : qzl, q2h = ax2 == 1 ? qyh : qzh;
@@ -478,15 +488,17 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemPar
 }
 
 // ---------------------------------------------------------------------------
-void launch_update_h(const AemParams& P, int counter, cudaStream_t s) {
+int launch_update_h(const AemParams& P, int counter, cudaStream_t s) {
     dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
     if (P.kmax) k_update_h<cf><<<grd, blk, 0, s>>>(P, counter);
     else k_update_h<float><<<grd, blk, 0, s>>>(P, counter);
+    return 1;
 }
-void launch_update_e(const AemParams& P, int counter, cudaStream_t s) {
+int launch_update_e(const AemParams& P, int counter, cudaStream_t s) {
     dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
     if (P.kmax) k_update_e<cf><<<grd, blk, 0, s>>>(P, counter);
     else k_update_e<float><<<grd, blk, 0, s>>>(P, counter);
+    return 1;
 }
 
 }  // namespace aem

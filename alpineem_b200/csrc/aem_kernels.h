@@ -1,4 +1,5 @@
-// aem_kernels.h -- launch interface of the per-step kernels.
+// aem_kernels.h -- launch interface of the per-step kernels (each launcher
+// returns the number of kernels it launched).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -39,13 +40,26 @@ struct FarFieldDev {
     float fac[3];               // area/(4 pi dt c) per face normal
     float wall_lo[3], wall_hi[3];
     const float* ang;           // per angle: sin(th), cos(th), sin(ph), cos(ph)
-    void* cur[3][2];            // per face normal / side: 8 arrays (4 new + 4 old) contiguous
+    void* cur[3][2];            // per face normal / side: the 4 current components of the last step
+    void* dbuf[3][2];           // per face: (new - old) of the 4 components, [comp][slot][cell], tb slots
     long long face_n[3];        // cells per face of that normal
     void* UW;                   // [6][nang][len]: Wx,Wy,Wz,Ux,Uy,Uz
     int mirror;                 // image-ground-plane pass
     float mir_off[3], use_mir[3], M_mir[3], J_mir[3];
     float kc3[3];               // kmax: k_count for Bloch-phase removal
+    // time-batched binning (FP32 path): tb steps of differences are kept and
+    // binned together; tb == 1 bins every step with the per-contribution kernel
+    int tb;
+    int nvang;                  // virtual angles: nang * (1 + mirror), image pass second
+    int hspan, group;           // histogram bins per (angle, component); angles per CTA
+    int tiles_u[3], tiles_v[3]; // 32x32 tiles per face of each normal
+    long long tile0[7];         // first tile of face (a, s) at index 2a+s
+    const float* kf;            // [nvang][3][2][3]: K0, Ku, Kv of the retarded-time offset tf(u, v)
+    int* err;                   // count of contributions that fell outside a histogram (must stay 0)
 };
+
+constexpr int FF_TB = 32;    // steps per far-field batch (one per warp lane)
+constexpr int FF_TILE = 32;  // face tile edge of the batched binning
 
 // per-step output taps
 struct TapDev {
@@ -65,12 +79,19 @@ struct TapDev {
     void* vid[6];               // Ex,Hx,Ey,Hy,Ez,Hz each (v1, v2, steps)
 };
 
-void launch_update_h(const AemParams& P, int counter, cudaStream_t s);
-void launch_update_e(const AemParams& P, int counter, cudaStream_t s);
-void launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
-void launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
-void launch_ff_currents(const AemParams& P, const FarFieldDev& F, cudaStream_t s);
-void launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s);
-void launch_taps(const AemParams& P, const TapDev& T, const FarFieldDev& F, int counter, int steps, cudaStream_t s);
+int launch_update_h(const AemParams& P, int counter, cudaStream_t s);
+int launch_update_e(const AemParams& P, int counter, cudaStream_t s);
+int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
+int launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
+int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaStream_t s);
+int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s);
+int launch_ff_bin_batch(const AemParams& P, const FarFieldDev& F, int n0, int nt, cudaStream_t s);
+size_t ff_batch_smem(const FarFieldDev& F);  // dynamic shared bytes of one batch CTA
+void ff_batch_prepare();                     // raise the kernel's shared-memory limit (once per device)
+// fused H+E step (aem_yee.cu): usable when the deck has none of TF/SF,
+// sheets, Drude poles, gridded ports, kmax
+bool yee_fused_ok(const AemParams& P, int gridded_ports);
+int launch_yee(const AemParams& P, cudaStream_t s);
+int launch_taps(const AemParams& P, const TapDev& T, const FarFieldDev& F, int counter, int steps, cudaStream_t s);
 
 }  // namespace aem

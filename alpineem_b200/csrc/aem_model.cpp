@@ -111,7 +111,7 @@ void edge_material(const HostModel& m, int comp, int i, int j, int k, float* eps
     }
 }
 
-void build_model(HostModel& m, const std::string& workdir) {
+void build_model(HostModel& m, const std::string& workdir, const float* bulk, size_t bulk_n) {
     Deck& d = m.d;
     const int N[3] = {d.X, d.Y, d.Z};
     for (int a = 0; a < 3; a++) m.S[a] = d.pbc[a] ? N[a] - 2 : N[a];
@@ -143,9 +143,10 @@ void build_model(HostModel& m, const std::string& workdir) {
 
     // geometry output (float32, (4,gx,gy,gz) column-major), ref :1963, :2355
     const int gx = N[0] - 1 - d.pbc[0], gy = N[1] - 1 - d.pbc[1], gz = N[2] - 1 - d.pbc[2];
-    m.geometry.assign((size_t)4 * gx * gy * gz, 0.0f);
+    if (d.ext_geometry_bin) m.geometry.assign((size_t)4 * gx * gy * gz, 0.0f);
+    else m.geometry.clear();
     auto geo = [&](int c, int i, int j, int k) -> float* {
-        if (i < 1 || j < 1 || k < 1 || i > gx || j > gy || k > gz) return nullptr;
+        if (m.geometry.empty() || i < 1 || j < 1 || k < 1 || i > gx || j > gy || k > gz) return nullptr;
         return &m.geometry[(((size_t)(k - 1) * gy + (j - 1)) * gx + (i - 1)) * 4 + c];
     };
     // a cell write the reference keeps: inside 1..N-1 and, on periodic axes,
@@ -161,12 +162,21 @@ void build_model(HostModel& m, const std::string& workdir) {
 
     m.cell_id.assign((size_t)m.cells, 0);
     if (!d.bulk_file.empty()) {  // ref :2051-2095
-        std::string path = resolve(workdir, d.bulk_file);
-        std::ifstream f(path, std::ios::binary);
-        if (!f) throw DeckError("cannot open bulk geometry file '" + path + "'");
-        std::vector<float> bg((size_t)gx * gy * gz);
-        f.read((char*)bg.data(), (std::streamsize)(bg.size() * sizeof(float)));
-        if ((size_t)f.gcount() != bg.size() * sizeof(float)) throw DeckError("bulk geometry file '" + path + "' is too short");
+        const size_t nbulk = (size_t)gx * gy * gz;
+        std::vector<float> file_data;
+        const float* bg = bulk;
+        if (bg) {
+            if (bulk_n != nbulk)
+                throw DeckError("bulk geometry has " + std::to_string(bulk_n) + " values, the grid needs " + std::to_string(nbulk));
+        } else {
+            std::string path = resolve(workdir, d.bulk_file);
+            std::ifstream f(path, std::ios::binary);
+            if (!f) throw DeckError("cannot open bulk geometry file '" + path + "'");
+            file_data.resize(nbulk);
+            f.read((char*)file_data.data(), (std::streamsize)(nbulk * sizeof(float)));
+            if ((size_t)f.gcount() != nbulk * sizeof(float)) throw DeckError("bulk geometry file '" + path + "' is too short");
+            bg = file_data.data();
+        }
         int mx = 0;
         for (auto& vm : d.mats) mx = std::max(mx, (int)vm.id);
         std::vector<int> tmp((size_t)mx + 1, 0);
@@ -178,7 +188,7 @@ void build_model(HostModel& m, const std::string& workdir) {
                     int iv = (int)v;
                     int mid = (iv >= 0 && iv <= mx) ? tmp[iv] : 0;
                     if (mid != 0) m.cell_id[m.lin(i, j, k)] = (uint8_t)mid;
-                    *geo(0, i, j, k) = v;
+                    if (float* g = geo(0, i, j, k)) *g = v;
                 }
     }
     int mid = 0;

@@ -54,7 +54,9 @@ struct HostModel {
 // Build the model: geometry rasterisation, material tables, sheets, Drude
 // boxes, CPML tables and gridded feeds.  `workdir` resolves relative file
 // names (bulk geometry, gridded feeds).  Throws DeckError.
-void build_model(HostModel& m, const std::string& workdir);
+// `bulk`, when not null, replaces the deck's bulk geometry file: `bulk_n`
+// float32 material ids in the file's layout (x fastest).
+void build_model(HostModel& m, const std::string& workdir, const float* bulk = nullptr, size_t bulk_n = 0);
 
 // Edge coefficients as the reference computes them from the averaged cell
 // properties (used by the host for sheet overrides and by tests).

@@ -6,9 +6,11 @@
 //   far-field currents and binning, plane sums, phase-centre, video.
 #include "aem_solver.h"
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 
@@ -20,6 +22,11 @@ namespace aem {
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + \
                                                         " at " #x);                                     \
     } while (0)
+
+static bool getenv_flag(const char* name) {
+    const char* v = std::getenv(name);
+    return v && *v && std::strcmp(v, "0") != 0;
+}
 
 static std::string dir_of(const std::string& p) {
     size_t s = p.find_last_of('/');
@@ -45,27 +52,88 @@ template <typename V>
 void* Solver::upload(const std::vector<V>& v) {
     void* p = alloc(v.size() * sizeof(V));
     if (!v.empty()) AEM_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, stream_));
+    h2d_bytes_ += v.size() * sizeof(V);
     return p;
 }
 
 Solver::Solver(const std::string& inputs_path, bool kmax, const std::string& outdir) : outdir_(outdir) {
-    AEM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     m_.d = parse_deck_file(inputs_path, kmax);
     derive(m_.d);
     build_model(m_, dir_of(inputs_path));
-    es_ = kmax ? 8 : 4;
-    setup_params();
-    setup_ports();
-    setup_farfield();
-    setup_taps();
-    AEM_CUDA(cudaStreamSynchronize(stream_));
+    init();
 }
 
-Solver::~Solver() {
+Solver::Solver(const std::string& deck_text, const std::string& ext_text, const float* bulk, size_t bulk_n, bool kmax,
+               const std::string& outdir, const std::string& workdir)
+    : outdir_(outdir) {
+    m_.d = parse_deck(deck_text, kmax);
+    apply_extensions(m_.d, ext_text);
+    derive(m_.d);
+    build_model(m_, workdir, bulk, bulk_n);
+    init();
+}
+
+void Solver::init() {
+    try {
+        AEM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        es_ = m_.d.kmax ? 8 : 4;
+        setup_params();
+        setup_ports();
+        setup_farfield();
+        setup_taps();
+        setup_fused();
+        AEM_CUDA(cudaStreamSynchronize(stream_));
+    } catch (...) {
+        release();  // a throwing constructor runs no destructor
+        throw;
+    }
+}
+
+// the fused H+E kernel needs second field and H-psi buffers (ping-pong)
+void Solver::setup_fused() {
+    int gridded = 0;
+    for (int q = 0; q < PS_.n; q++) gridded += PS_.p[q].gridded;
+    // a port whose cells or H loop reach a CPML slab sees the fields between
+    // the bulk pass and the CPML pass, as in the reference (ports_h before
+    // cpml_h, ports_e before cpml_e, ref :4797-5375 / :6120-6670)
+    const Deck& dk = m_.d;
+    const int N[3] = {dk.X, dk.Y, dk.Z};
+    split_ = false;
+    for (const Port& pt : dk.ports) {
+        if (pt.gridded) { split_ = true; continue; }  // feed planes: keep the reference order always
+        for (int a = 0; a < 3; a++) {
+            if (dk.pbc[a]) continue;
+            const int lo = (int)pt.loc[a] - 1, hi = (int)pt.loc[a] + (int)pt.size[a];
+            if (lo <= dk.npml[a][0] || hi >= N[a] + 1 - dk.npml[a][1]) split_ = true;
+        }
+    }
+    fused_ = yee_fused_ok(P_, gridded) && !split_ && !getenv_flag("AEM_TWO_KERNEL");
+    if (!fused_) return;
+    for (int c = 0; c < 3; c++) {
+        P_.E2[c] = alloc((size_t)m_.cells * es_);
+        P_.H2[c] = alloc((size_t)m_.cells * es_);
+    }
+    for (int c = 0; c < 3; c++)
+        for (int a = 0; a < 3; a++)
+            for (int s = 0; s < 2; s++) {
+                if (!P_.psi_h[c][a][s]) continue;
+                int n = dk.npml[a][s];
+                size_t e0 = a == 0 ? n : P_.PX, e1 = a == 1 ? n : P_.SY, e2 = a == 2 ? n : P_.SZ;
+                P_.psi_h2[c][a][s] = alloc(e0 * e1 * e2 * es_);
+            }
+}
+
+void Solver::release() {
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : bufs_) cudaFree(p);
+    bufs_.clear();
+    for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
+    prof_pool_.clear();
     if (stream_) cudaStreamDestroy(stream_);
+    stream_ = nullptr;
 }
+
+Solver::~Solver() { release(); }
 
 long long Solver::cell_count() const {
     const Deck& d = m_.d;
@@ -340,10 +408,11 @@ void Solver::setup_farfield() {
         // faces, as the reference's loops over it are empty
         const long long nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
         F.face_n[a] = (F.has[a] && nb > 0 && nc > 0 && F.hi[a] >= F.lo[a]) ? nb * nc : 0;
-        for (int s = 0; s < 2; s++)
-            if (F.has[a]) F.cur[a][s] = alloc((size_t)F.face_n[a] * 8 * es_);
+        F.tiles_u[a] = F.face_n[a] ? (int)((nb + FF_TILE - 1) / FF_TILE) : 0;
+        F.tiles_v[a] = F.face_n[a] ? (int)((nc + FF_TILE - 1) / FF_TILE) : 0;
     }
     F.mirror = (d.is_mirror && d.pbc[0] + d.pbc[1] + d.pbc[2] < 2 && !d.kmax) ? 1 : 0;
+    F.nvang = F.nang * (1 + F.mirror);
     std::vector<float> ang((size_t)4 * F.nang);
     for (int q = 0; q < F.nang; q++) {
         ang[4 * q + 0] = std::sin(d.ff_theta[q]);
@@ -353,6 +422,59 @@ void Solver::setup_farfield() {
     }
     F.ang = (const float*)upload(ang);
     F.UW = alloc((size_t)6 * F.nang * F.len * es_);
+    F.err = (int*)alloc(sizeof(int));
+
+    // retarded-time offset of face cell (u, v) for virtual angle va (image
+    // pass second): tf = (r_relay - sum_e (pos_e - centre_e) del_e dir_e) / (c dt)
+    // with pos the cell's reference index (mirrored in the image pass,
+    // ref :7958-8230), written as K0 + Ku u + Kv v
+    std::vector<float> kf((size_t)F.nvang * 3 * 2 * 3, 0.0f);
+    double span = 0;
+    const int ctr[3] = {F.ic, F.jc, F.kc};
+    for (int va = 0; va < F.nvang; va++) {
+        const int q = va % F.nang, pass = va / F.nang;
+        const double dir[3] = {(double)ang[4 * q] * ang[4 * q + 3], (double)ang[4 * q] * ang[4 * q + 2], (double)ang[4 * q + 1]};
+        for (int a = 0; a < 3; a++) {
+            const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+            for (int s = 0; s < 2; s++) {
+                // pos_e = sg_e * idx_e + of_e
+                double sg[3], of[3];
+                for (int e = 0; e < 3; e++) {
+                    const bool m = pass && F.use_mir[e] != 0.0f;
+                    sg[e] = m ? -1.0 : 1.0;
+                    of[e] = m ? (double)F.mir_off[e] : 0.0;
+                }
+                int idx0[3];
+                idx0[a] = s ? F.hi[a] : F.lo[a];
+                idx0[b] = F.lo[b];
+                idx0[c] = F.lo[c];
+                double proj0 = 0;
+                for (int e = 0; e < 3; e++) proj0 += (sg[e] * idx0[e] + of[e] - ctr[e]) * (double)dl[e] * dir[e];
+                float* k = &kf[(((size_t)va * 3 + a) * 2 + s) * 3];
+                k[0] = (float)(((double)F.r_relay - proj0) / (double)F.c_dt);
+                k[1] = (float)(-sg[b] * (double)dl[b] * dir[b] / (double)F.c_dt);
+                k[2] = (float)(-sg[c] * (double)dl[c] * dir[c] / (double)F.c_dt);
+                if (F.face_n[a]) span = std::max(span, std::fabs((double)k[1]) * (FF_TILE - 1) + std::fabs((double)k[2]) * (FF_TILE - 1));
+            }
+        }
+    }
+    // time batching on the FP32 path when the histograms fit in shared memory
+    F.hspan = (int)std::ceil(span) + FF_TB + 8;
+    const size_t smem_max = 96 * 1024;
+    F.group = (int)std::min<size_t>(64, smem_max / ((size_t)4 * F.hspan * sizeof(float)));
+    F.tb = (!d.kmax && F.group >= 1) ? FF_TB : 1;
+    if (F.tb > 1) {
+        F.kf = (const float*)upload(kf);
+        F.tile0[0] = 0;
+        for (int f = 0; f < 6; f++) F.tile0[f + 1] = F.tile0[f] + (long long)F.tiles_u[f >> 1] * F.tiles_v[f >> 1];
+        ff_batch_prepare();
+    }
+    for (int a = 0; a < 3; a++)
+        for (int s = 0; s < 2; s++)
+            if (F.has[a]) {
+                F.cur[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
+                F.dbuf[a][s] = alloc((size_t)F.face_n[a] * 4 * F.tb * es_);
+            }
 }
 
 void Solver::setup_taps() {
@@ -393,14 +515,124 @@ void Solver::setup_taps() {
     }
 }
 
+// run one launcher; with profiling on, bracket it with events on the stream
+template <typename Fn>
+void Solver::phase(int ph, Fn&& fn) {
+    if (!prof_on_) {
+        launches_ += fn();
+        return;
+    }
+    cudaEvent_t e0 = prof_event(), e1 = prof_event();
+    AEM_CUDA(cudaEventRecord(e0, stream_));
+    const int n = fn();
+    AEM_CUDA(cudaEventRecord(e1, stream_));
+    launches_ += n;
+    if (n) prof_marks_.push_back({ph, n, e0, e1});
+}
+
+cudaEvent_t Solver::prof_event() {
+    if (prof_used_ == prof_pool_.size()) {
+        cudaEvent_t e;
+        AEM_CUDA(cudaEventCreate(&e));
+        prof_pool_.push_back(e);
+    }
+    return prof_pool_[prof_used_++];
+}
+
+void Solver::set_profiling(bool on) {
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    prof_on_ = on;
+    prof_used_ = 0;
+    prof_marks_.clear();
+}
+
+void Solver::read_profile(double ms[AEM_NPHASE], long long launches[AEM_NPHASE]) {
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    for (int p = 0; p < AEM_NPHASE; p++) { ms[p] = 0; launches[p] = 0; }
+    for (const ProfMark& m : prof_marks_) {
+        float t = 0;
+        AEM_CUDA(cudaEventElapsedTime(&t, m.e0, m.e1));
+        ms[m.phase] += t;
+        launches[m.phase] += m.n;
+    }
+}
+
+void Solver::read_probe(int kind, int index, int first, int n, double* re, double* im) {
+    const void* src = nullptr;
+    if (kind == 5) {
+        if (index < 0 || index >= PS_.n) throw std::invalid_argument("no such port");
+        src = PS_.p[index].vout;
+    } else if (kind == 1 || kind == 2) {
+        if (!TP_.plane_sum) throw std::invalid_argument("the deck has no reflection/transmission planes");
+        src = kind == 1 ? TP_.refl : TP_.trans;
+    } else {
+        throw std::invalid_argument("probe kind must be 1, 2 or 5");
+    }
+    if (first < 1 || n < 0 || first - 1 + n > done_) throw std::invalid_argument("steps outside those run so far");
+    std::vector<char> buf((size_t)n * es_);
+    AEM_CUDA(cudaMemcpyAsync(buf.data(), (const char*)src + (size_t)(first - 1) * es_, buf.size(), cudaMemcpyDeviceToHost, stream_));
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    d2h_bytes_ += buf.size();
+    for (int q = 0; q < n; q++) {
+        if (es_ == 4) {
+            re[q] = ((const float*)buf.data())[q];
+            if (im) im[q] = 0;
+        } else {
+            re[q] = ((const float*)buf.data())[2 * q];
+            if (im) im[q] = ((const float*)buf.data())[2 * q + 1];
+        }
+    }
+}
+
 void Solver::step(int counter) {
-    launch_update_h(P_, counter, stream_);
-    launch_ports_h(P_, PS_, counter, stream_);
-    launch_update_e(P_, counter, stream_);
-    launch_ports_e(P_, PS_, counter, stream_);
-    launch_ff_currents(P_, FF_, stream_);
-    launch_ff_bin(P_, FF_, counter, stream_);
-    launch_taps(P_, TP_, FF_, counter, m_.d.steps, stream_);
+    if (fused_) {
+        // H and E in one pass into the second buffers, then swap; the basic
+        // ports read H_new and overwrite E_new exactly as between and after
+        // the reference's two half-steps
+        phase(AEM_PHASE_YEE, [&] { return launch_yee(P_, stream_); });
+        for (int c = 0; c < 3; c++) {
+            std::swap(P_.E[c], P_.E2[c]);
+            std::swap(P_.H[c], P_.H2[c]);
+            for (int a = 0; a < 3; a++)
+                for (int s = 0; s < 2; s++) std::swap(P_.psi_h[c][a][s], P_.psi_h2[c][a][s]);
+        }
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_h(P_, PS_, counter, stream_); });
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_e(P_, PS_, counter, stream_); });
+    } else if (split_) {
+        AemParams& P1 = split_params_[0];
+        AemParams& P2 = split_params_[1];
+        P1 = P_; P1.cpml_split = 1;
+        P2 = P_; P2.cpml_split = 2;
+        phase(AEM_PHASE_UPDATE_H, [&] { return launch_update_h(P1, counter, stream_); });
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_h(P_, PS_, counter, stream_); });
+        phase(AEM_PHASE_UPDATE_H, [&] { return launch_update_h(P2, counter, stream_); });
+        phase(AEM_PHASE_UPDATE_E, [&] { return launch_update_e(P1, counter, stream_); });
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_e(P_, PS_, counter, stream_); });
+        phase(AEM_PHASE_UPDATE_E, [&] { return launch_update_e(P2, counter, stream_); });
+    } else {
+        phase(AEM_PHASE_UPDATE_H, [&] { return launch_update_h(P_, counter, stream_); });
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_h(P_, PS_, counter, stream_); });
+        phase(AEM_PHASE_UPDATE_E, [&] { return launch_update_e(P_, counter, stream_); });
+        phase(AEM_PHASE_PORTS, [&] { return launch_ports_e(P_, PS_, counter, stream_); });
+    }
+    if (FF_.tb > 1) {
+        // differences go to slot counter - ff_n0_; a full batch is binned at once
+        phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, counter - ff_n0_, stream_); });
+        if (counter - ff_n0_ + 1 == FF_.tb) flush_farfield(counter);
+    } else {
+        phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, 0, stream_); });
+        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin(P_, FF_, counter, stream_); });
+    }
+    phase(AEM_PHASE_TAPS, [&] { return launch_taps(P_, TP_, FF_, counter, m_.d.steps, stream_); });
+}
+
+// bin the steps ff_n0_..last held in the difference buffer
+void Solver::flush_farfield(int last) {
+    if (FF_.tb > 1 && last >= ff_n0_) {
+        const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
+        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_batch(P_, FF_, n0, nt, stream_); });
+    }
+    ff_n0_ = last + 1;
 }
 
 void Solver::run(int n) {
@@ -408,6 +640,9 @@ void Solver::run(int n) {
         done_++;
         step(done_);
     }
+    // the last step bins whatever the batch buffer still holds; earlier
+    // partial batches wait for more steps (or for flush())
+    if (done_ == m_.d.steps) flush_farfield(done_);
     AEM_CUDA(cudaGetLastError());
 }
 

@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/alpineem_b200.h"  // AEM_PHASE_*
 #include "aem_kernels.h"
 #include "aem_model.h"
 
@@ -21,6 +22,10 @@ class Solver {
     // Parse `inputs_path` (relative files resolve against its directory),
     // build the model and upload it to the current CUDA device.
     Solver(const std::string& inputs_path, bool kmax, const std::string& outdir);
+    // Same from memory: the deck text, extension lines, and the bulk
+    // geometry values when the deck names a bulk file (else null).
+    Solver(const std::string& deck_text, const std::string& ext_text, const float* bulk, size_t bulk_n, bool kmax,
+           const std::string& outdir, const std::string& workdir);
     ~Solver();
     Solver(const Solver&) = delete;
     Solver& operator=(const Solver&) = delete;
@@ -38,6 +43,21 @@ class Solver {
     int steps_done() const { return done_; }
     size_t device_bytes() const { return dev_bytes_; }
     cudaStream_t stream() const { return stream_; }
+    bool fused() const { return fused_; }
+    // kernels launched so far
+    long long launches() const { return launches_; }
+    // bytes copied host->device (model upload) and device->host so far
+    size_t h2d_bytes() const { return h2d_bytes_; }
+    size_t d2h_bytes() const { return d2h_bytes_; }
+    // bin far-field contributions still held in the batch buffer
+    void flush() { flush_farfield(done_); }
+    // per-phase device time: with profiling on, every launcher is bracketed
+    // by CUDA events on the solver's stream; read_profile sums them
+    void set_profiling(bool on);
+    void read_profile(double ms[AEM_NPHASE], long long launches[AEM_NPHASE]);
+    // raw per-step samples on the device: port voltage (kind 5, Voltage_out)
+    // or unnormalised plane sums (kind 1 reflected, 2 transmitted)
+    void read_probe(int kind, int index, int first, int n, double* re, double* im);
     // bytes the fused Yee/CPML update must move per step (algorithmic)
     double algorithmic_bytes_per_step() const;
     long long cell_count() const;
@@ -52,6 +72,8 @@ class Solver {
     std::vector<double> pc_re[3], pc_im[3];
 
    private:
+    void init();
+    void release();
     void* alloc(size_t bytes);
     template <typename V>
     void* upload(const std::vector<V>& v);
@@ -59,7 +81,12 @@ class Solver {
     void setup_ports();
     void setup_farfield();
     void setup_taps();
+    void setup_fused();
     void step(int counter);
+    void flush_farfield(int last);
+    template <typename Fn>
+    void phase(int ph, Fn&& fn);
+    cudaEvent_t prof_event();
 
     std::string outdir_;
     HostModel m_;
@@ -71,6 +98,20 @@ class Solver {
     size_t dev_bytes_ = 0;
     int es_ = 4;  // bytes per field value
     int done_ = 0;
+    bool fused_ = false;  // one fused H+E kernel per step (k_yee)
+    bool split_ = false;  // bulk / port / CPML passes (a port inside a CPML slab)
+    AemParams split_params_[2];
+    int ff_n0_ = 1;  // first step held in the far-field difference buffer
+    long long launches_ = 0;
+    size_t h2d_bytes_ = 0, d2h_bytes_ = 0;
+    struct ProfMark {
+        int phase, n;
+        cudaEvent_t e0, e1;
+    };
+    bool prof_on_ = false;
+    std::vector<cudaEvent_t> prof_pool_;
+    size_t prof_used_ = 0;
+    std::vector<ProfMark> prof_marks_;
     cudaStream_t stream_ = nullptr;
 };
 

@@ -115,4 +115,13 @@ struct AemParams {
     // kmax plane source
     int kmax_src_axis, kmax_mode_TE, kmax_mode_TM, k_pl_H, k_pl_E;
     float kcnt[3], knum[3], two_pi_f;
+    // 0: update kernels apply bulk and CPML together; 1: bulk only; 2: CPML
+    // only (a port inside a CPML slab needs the reference's order: bulk,
+    // port half-step, CPML pass)
+    int cpml_split;
+    // fused H+E step (k_yee): the new fields and H-psi go to these buffers
+    // (ping-pong with E/H/psi_h above; the host swaps them after each step)
+    void* E2[3];
+    void* H2[3];
+    void* psi_h2[3][3][2];
 };

@@ -1,0 +1,66 @@
+"""Synthetic workloads in the reference's input grammar.
+
+The reference ships no benchmark decks; these builders generate the
+throughput workloads from seeded random draws, as decks for
+alpineem_b200.deck plus a bulk-geometry array (the contents of the
+reference's optional_geom_bulk.bin, main_fdtd/fdtd_solver.f90:2051-2095:
+float32 material ids, x fastest).
+"""
+import numpy as np
+
+
+def _ellipsoids(bulk, n_ell, rng, semi, eps_range, lo, hi, first_id):
+    """Rasterise axis-aligned ellipsoids into `bulk` (shape (nz, ny, nx)).
+    Cell (i, j, k) (1-based) is inside when its centre (i-0.5, ...) lies in
+    the ellipsoid.  Returns the material list entries."""
+    nz, ny, nx = bulk.shape
+    mats = []
+    for e in range(n_ell):
+        mid = first_id + e
+        eps = float(rng.uniform(*eps_range))
+        ax = rng.uniform(semi[0], semi[1], size=3)  # semi-axes x, y, z in cells
+        c = np.array([rng.uniform(lo[a], hi[a]) for a in range(3)])
+        mats.append(("simple", mid, (eps, eps, eps), (0, 0, 0)))
+        b0 = [max(1, int(np.floor(c[a] - ax[a]))) for a in range(3)]
+        b1 = [min((nx, ny, nz)[a], int(np.ceil(c[a] + ax[a])) + 1) for a in range(3)]
+        i = np.arange(b0[0], b1[0] + 1) - 0.5
+        j = np.arange(b0[1], b1[1] + 1) - 0.5
+        k = np.arange(b0[2], b1[2] + 1) - 0.5
+        r = (((k[:, None, None] - c[2]) / ax[2]) ** 2 + ((j[None, :, None] - c[1]) / ax[1]) ** 2 +
+             ((i[None, None, :] - c[0]) / ax[0]) ** 2)
+        sl = bulk[b0[2] - 1:b1[2], b0[1] - 1:b1[1], b0[0] - 1:b1[0]]
+        sl[r <= 1.0] = mid
+    return mats
+
+
+def dipole_ellipsoids(n=1024, steps=4000, n_ell=64, seed=2, pml_cells=16, dl="2E-3", f="5E9",
+                      theta_step=10, phi_step=10, arm=30, semi=(5, 40)):
+    """Large single-GPU throughput run: an n^3 grid (spacing dl) with
+    `pml_cells` of CPML on every face, a z-directed dipole of two 1x1x`arm`
+    PEC arms around a 1-cell 50-ohm basic lumped port driven by a Gaussian
+    pulse, `n_ell` dielectric ellipsoids (eps_r ~ U[2,12], semi-axes ~
+    U[semi] cells scaled by n/1024, centres ~ U over the interior, numpy
+    default_rng(seed)), and time-domain far fields on a theta_step x
+    phi_step degree grid (theta 0..180, phi 0..360-phi_step).
+
+    Returns (deck, ext_text, bulk): the deck as a dict for
+    alpineem_b200.deck.deck_text, the extension lines, and bulk of shape
+    (n, n, n) float32.
+    """
+    rng = np.random.default_rng(seed)
+    scale = n / 1024.0
+    bulk = np.zeros((n, n, n), np.float32)
+    lo = [pml_cells + 4] * 3
+    hi = [n - pml_cells - 4] * 3
+    mats = [("simple", 1, (1, 1, 1), ("1E8", "1E8", "1E8"))]
+    mats += _ellipsoids(bulk, n_ell, rng, (semi[0] * scale, semi[1] * scale), (2.0, 12.0), lo, hi, first_id=2)
+    c = n // 2
+    arm = max(1, min(arm, c - pml_cells - 3))
+    ff = [(t, p) for t in range(0, 181, theta_step) for p in range(0, 360, phi_step)]
+    d = dict(n=(n, n, n), dl=(dl, dl, dl), steps=steps, factor=1, f=f, pulse=1, bc=(0, 0, 0, 0, 0, 0),
+             excitation=("antenna", 1, 0, 1), ff=ff, ffc=(c, c, c), name="data.dat", mats=mats,
+             bulk="optional_geom_bulk.bin",
+             objects=[("block", 1, (c, c, c - arm), (1, 1, arm)), ("block", 1, (c, c, c + 1), (1, 1, arm))],
+             ports=[("basic", "z", 50, (c, c, c), (1, 1, 1))])
+    ext = "pml_cells %d\ngeometry_bin no\n" % pml_cells
+    return d, ext, bulk

@@ -50,9 +50,76 @@ int aem_version(void);
  * reference).  Writes <name>_geometry.bin as the reference does. */
 int aem_create_from_file(const char* inputs_path, int mode, const char* outdir, aem_handle** out);
 
+/* Same as aem_create_from_file with the inputs in caller memory (copied
+ * in): `deck_text` is the inputs.txt text (fdtd_solver.f90:726-1298
+ * grammar); `ext_text` (may be NULL) holds extension lines, one "key value"
+ * per line, as in the optional "<inputs>.b200" sidecar:
+ *   pml_cells N      CPML thickness in cells (reference: 10, :1305-1318)
+ *   geometry_bin no  skip building and writing <name>_geometry.bin
+ * `bulk` replaces the bulk geometry file the deck names (:2051-2055):
+ * bulk_count float32 material ids, x fastest, (nx, ny, nz) cells; NULL/0
+ * when the deck has none.  Side files (gridded feeds) and outputs resolve
+ * against `outdir`.  The reference reads these inputs from disk only. */
+int aem_create_from_memory(const char* deck_text, const char* ext_text, const float* bulk, size_t bulk_count,
+                           int mode, const char* outdir, aem_handle** out);
+
+/* Parse and validate a deck (and extension lines) without a GPU, returning
+ * the reference grid sizes X, Y, Z (fdtd_solver.f90:1316-1318).  Fails with
+ * AEM_ERR_INPUT and the reference's "ERROR: ..." text where the reference
+ * stops (:726-1298). */
+int aem_check_deck(const char* deck_text, const char* ext_text, int mode, int sizes[3]);
+
 /* Advance `nsteps` time steps of the reference loop (fdtd_solver.f90:4440,
  * one `counter` per step), never past the deck's step count. */
 int aem_run(aem_handle* h, int nsteps);
+
+/* Raw per-step samples of the steps run so far, before the normalisation
+ * that aem_write_outputs applies: kind 5 = voltage of port `index`
+ * (Voltage_out, fdtd_solver.f90:8241-8243), kind 1 / 2 = reflected /
+ * transmitted plane sums (:7005-7103).  Steps first_step .. first_step+n-1
+ * (1-based); im may be NULL.  Synchronises the handle's stream. */
+int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, double* re, double* im);
+
+/* Phases of a time step, for per-phase device timing. */
+#define AEM_NPHASE 8
+#define AEM_PHASE_UPDATE_H 0     /* H update with sheets, TF/SF, CPML, PBC */
+#define AEM_PHASE_UPDATE_E 1     /* E update with sheets, Drude, TF/SF, CPML, PBC */
+#define AEM_PHASE_PORTS 2        /* lumped-port half-steps */
+#define AEM_PHASE_FF_CURRENTS 3  /* Huygens-surface currents */
+#define AEM_PHASE_FF_BIN 4       /* retarded-time binning */
+#define AEM_PHASE_TAPS 5         /* plane sums, phase-centre, video */
+#define AEM_PHASE_YEE 6          /* fused H+E update (decks without TF/SF, sheets, Drude, kmax) */
+#define AEM_PHASE_OTHER 7
+
+/* Per-phase timing (an extension; the reference prints only a total):
+ * with profiling on, each kernel launch is bracketed by CUDA events on the
+ * handle's stream.  aem_profile(h, 1) clears the record;
+ * aem_profile_read returns milliseconds and launches per phase since. */
+int aem_profile(aem_handle* h, int enable);
+int aem_profile_read(aem_handle* h, double ms[AEM_NPHASE], long long launches[AEM_NPHASE]);
+
+/* Kernels launched by the handle so far. */
+int aem_launch_count(aem_handle* h, long long* n);
+
+/* The far-field binning runs once per 32 steps over the buffered surface
+ * currents (same sums as the reference's per-step binning,
+ * fdtd_solver.f90:7643-7925); aem_flush bins the steps still buffered.
+ * aem_write_outputs and the last step of the deck flush by themselves. */
+int aem_flush(aem_handle* h);
+
+/* The CUDA stream (cudaStream_t) the handle launches on, so callers can
+ * order their own work and events after it. */
+int aem_stream(aem_handle* h, void** stream);
+
+/* Bytes copied host->device (model upload) and device->host (outputs,
+ * probes, fields) by the handle so far. */
+int aem_transfer_bytes(aem_handle* h, long long* h2d, long long* d2h);
+
+/* Cells updated per step, (X-1)(Y-1)(Z-1) as the reference counts them
+ * (fdtd_solver.f90:8315-8316), and the algorithmic HBM bytes one step must
+ * move: 12 field values read + written and 1 material byte per cell, plus
+ * 8 CPML psi values per cell of each CPML slab. */
+int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step);
 
 /* Steps done so far and the deck's step count. */
 int aem_steps(aem_handle* h, int* done, int* total);

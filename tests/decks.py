@@ -4,112 +4,7 @@ one per solver feature, sized so the CPU oracle finishes each in seconds.
 Used by the GPU parity tests and smoke()."""
 import os
 
-
-def deck_text(d):
-    L = []
-    w = L.append
-    w("%d,%d,%d" % tuple(d["n"]))
-    w("%s,%s,%s" % tuple(d.get("dl", ("1E-3", "1E-3", "1E-3"))))
-    w(str(d["steps"]))
-    w(str(d.get("factor", 1)))
-    w(str(d.get("f", "10E9")))
-    w(str(d.get("pulse", 2)))
-    w(",".join(str(b) for b in d.get("bc", (0, 0, 0, 0, 0, 0))))
-    if "igp" in d:
-        w("IGP")
-        w(d["igp"][0])
-        w(str(d["igp"][1]))
-    else:
-        w("none")
-    ex = d["excitation"]
-    if ex[0] == "plane wave":
-        w("plane wave")
-        w("%s,%s" % (ex[1], ex[2]))
-        if d.get("kmax"):
-            w(ex[3])  # TE / TM
-            w(ex[4])  # + / -
-        else:
-            w("%s,%s,%s" % tuple(ex[3:6]))
-    else:
-        w("antenna")
-        w("%s,%s" % (ex[1], ex[2]))
-        w(str(ex[3]))
-    if d.get("kmax"):
-        w("%s,%s" % tuple(d["k"]))
-    ff = d.get("ff", [])
-    w(str(len(ff)))
-    if ff:
-        w("%d,%d,%d" % tuple(d["ffc"]))
-        for t, p in ff:
-            w("%s,%s" % (t, p))
-    if "video" in d:
-        w("yes")
-        w(d["video"][0])
-        w(str(d["video"][1]))
-    else:
-        w("no")
-    w(d.get("full", "no"))
-    w(d.get("name", "data.dat"))
-    mats = d.get("mats", [])
-    w(str(len(mats)))
-    for m in mats:
-        if m[0] == "sheet":
-            w("sheet")
-            w(str(m[1]))
-            w(str(m[2]))
-        else:
-            w("volume")
-            w(m[0])  # simple / plasma
-            w(str(m[1]))
-            w("%s,%s,%s" % tuple(m[2]))
-            w("%s,%s,%s" % tuple(m[3]))
-            if m[0] == "plasma":
-                w(str(len(m[4])))
-                for wp, gm in m[4]:
-                    w("%s,%s,%s" % (wp, wp, wp))
-                    w("%s,%s,%s" % (gm, gm, gm))
-    if "bulk" in d:
-        w("yes")
-        w(d["bulk"])
-    else:
-        w("no")
-    objs = d.get("objects", [])
-    w(str(len(objs)))
-    for o in objs:
-        w(o[0])
-        w(str(o[1]))
-        if o[0] == "block":
-            w("%d,%d,%d" % tuple(o[2]))
-            w("%d,%d,%d" % tuple(o[3]))
-        elif o[0] == "sphere":
-            w("%d,%d,%d" % tuple(o[2]))
-            w(str(o[3]))
-        else:
-            w(o[2])
-            w("%d,%d,%d" % tuple(o[3]))
-            w("%d,%d" % tuple(o[4]))
-    sheets = d.get("sheets", [])
-    w(str(len(sheets)))
-    for s in sheets:
-        w(s[0])
-        w(str(s[1]))
-        w(str(s[2]))
-        w("%d,%d" % tuple(s[3]))
-        w("%d,%d" % tuple(s[4]))
-    ports = d.get("ports", [])
-    w(str(len(ports)))
-    for p in ports:
-        w(p[0])
-        w(p[1])
-        w(str(p[2]))
-        w("%d,%d,%d" % tuple(p[3]))
-        if p[0] == "basic":
-            w("%d,%d,%d" % tuple(p[4]))
-        else:
-            w("%d,%d" % tuple(p[4]))
-            w(p[5])
-    w("0")
-    return "\n".join(L) + "\n"
+from alpineem_b200.deck import deck_text  # noqa: F401  (re-exported for the tests)
 
 
 ANG = [(0, 0), (45, 30), (90, 180), (135, 270), (180, 0)]
@@ -168,12 +63,60 @@ DECKS = {
                     excitation=("plane wave", 1, 0, "TM", "-"), k=("0.0", "250.0"),
                     mats=[("simple", 5, (4, 4, 4), (0.02, 0.02, 0.02))],
                     objects=[("block", 5, (14, 1, 1), (8, 10, 10))]),
+    # --- decks of the fused H+E kernel (no TF/SF, sheets, Drude or kmax) ---
+    # x-periodic array of dipoles between lossy dielectric blocks; 2 CTAs in
+    # x (wrap across them), several in y, far field on the y and z faces
+    "dipole_pbc_x": dict(n=(40, 30, 34), steps=240, f="15E9", pulse=1, bc=(1, 1, 0, 0, 0, 0),
+                         excitation=("antenna", 1, 0, 1), ff=[(90, 0), (60, 90), (30, 200)], ffc=(20, 15, 17),
+                         mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (3, 2, 4), (0.01, 0, 0.02))],
+                         objects=[("block", 4, (20, 15, 12), (1, 1, 5)), ("block", 4, (20, 15, 18), (1, 1, 5)),
+                                  ("sphere", 5, (9, 10, 20), 5), ("block", 5, (30, 4, 8), (12, 6, 6))],
+                         ports=[("basic", "z", 50, (20, 15, 17), (1, 1, 1))]),
+    # long z-periodic column whose port lies inside the y CPML slabs: the
+    # bulk / port / CPML pass order of the reference
+    "dipole_long_z": dict(n=(24, 20, 150), steps=200, f="15E9", pulse=1, bc=(0, 0, 0, 0, 1, 1),
+                          excitation=("antenna", 1, 0, 1),
+                          mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 6, (5, 5, 5), (0, 0, 0))],
+                          objects=[("block", 4, (12, 10, 60), (1, 1, 6)), ("block", 4, (12, 10, 67), (1, 1, 6)),
+                                   ("cylinder", 6, "z", (12, 10, 100), (40, 3))],
+                          ports=[("basic", "z", 50, (12, 10, 66), (1, 1, 1))]),
+    # z-periodic column wide enough to keep the port out of the CPML: three
+    # z chunks of the fused kernel, the first recomputing the H plane across
+    # the periodic wrap
+    "fused_long_z": dict(n=(40, 36, 150), steps=200, f="15E9", pulse=1, bc=(0, 0, 0, 0, 1, 1),
+                         excitation=("antenna", 1, 0, 1),
+                         mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 6, (5, 5, 5), (0, 0, 0))],
+                         objects=[("block", 4, (20, 18, 60), (1, 1, 6)), ("block", 4, (20, 18, 67), (1, 1, 6)),
+                                  ("cylinder", 6, "z", (20, 18, 100), (40, 3))],
+                         ports=[("basic", "z", 50, (20, 18, 66), (1, 1, 1))]),
+    # the throughput workload at 48^3: bulk-file ellipsoids, 6-cell CPML
+    # (sidecar), a 1-cell port and 56 far-field angles
+    "ellipsoids_small": "ellipsoids_small",
 }
 
 
+def _ellipsoids_small():
+    from alpineem_b200 import workloads
+    d, ext, bulk = workloads.dipole_ellipsoids(n=48, steps=260, n_ell=6, seed=2, pml_cells=6, dl="1E-3", f="20E9",
+                                               theta_step=30, phi_step=45, arm=8, semi=(64, 256))
+    d["_ext"] = ext.replace("geometry_bin no\n", "")
+    d["_bulk"] = bulk
+    return d
+
+
+DECKS["ellipsoids_small"] = _ellipsoids_small()
+
+
 def write_deck(name, directory, fname="inputs.txt"):
+    """Write deck `name` (and its sidecar / bulk geometry file, if any) into
+    `directory`; returns (path, kmax)."""
     d = DECKS[name]
     path = os.path.join(directory, fname)
     with open(path, "w") as f:
         f.write(deck_text(d))
+    if "_ext" in d:
+        with open(path + ".b200", "w") as f:
+            f.write(d["_ext"])
+    if "_bulk" in d:
+        d["_bulk"].tofile(os.path.join(directory, d["bulk"]))
     return path, bool(d.get("kmax"))
