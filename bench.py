@@ -1,0 +1,323 @@
+"""bench.py -- FDTD time-step throughput of the B200 solver.
+
+Workload "dipole_ellipsoids": a 1024^3 grid (2 mm cells, 16-cell CPML on
+every face) with a 60-cell z dipole fed by a 1-cell 50-ohm lumped port
+(Gaussian pulse), 64 random dielectric ellipsoids (eps_r ~ U[2,12],
+semi-axes ~ U[5,40] cells, numpy default_rng(2)) given as a bulk geometry
+array, and time-domain far fields at 684 angles (10 x 10 degree theta/phi
+grid); deck length 4000 steps (alpineem_b200/workloads.py).  One bench step
+is one full FDTD time step of that deck: H and E updates with CPML, the
+port half-steps, the Huygens-surface currents and the retarded-time binning
+of all 684 angles (binned once per 32 steps over the buffered currents).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is Mcell-updates/s, cells counted as the reference does
+((X-1)(Y-1)(Z-1) per step): K steps timed with CUDA events on the solver's
+stream, inputs resident on the device (28 GB of fields and tables, far above
+the 126 MB L2, so no L2 flush is needed).  With N > 1 (torchrun) every rank
+runs an independent replica (a single grid is not split across GPUs) and
+the value is the sum of the ranks' cell-updates over the slowest rank's
+time.  `e2e` times a complete K-step job through the C ABI from host
+buffers: model upload, K steps each followed by a device->host read of that
+step's port voltage, and the output files.  `--impl reference` times the
+CPU oracle (a C/OpenMP restatement of the reference's Fortran loop) on a
+256^3 sample of the same workload on all host threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FDTD Mcell-updates/s"
+UNIT = "Mcell-updates/s"
+WORKLOAD = "dipole_ellipsoids"
+FALLBACK_HBM_GBS = 6650.0
+ORACLE = os.path.join(ROOT, "oracle", "_build", "fdtd_oracle")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=96)
+    ap.add_argument("--warmup", type=int, default=32)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1024, help="grid cells per axis of the GPU workload")
+    ap.add_argument("--cpu-n", type=int, default=256, help="grid cells per axis of the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=8, help="timed steps of the cpu_baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def ranks():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dram_traffic_per_cell():
+    """Per-cell-update DRAM bytes of the Yee update from the committed ncu
+    summary (profiles/yee_update_dipole_ellipsoids.md, line
+    'dram_bytes_per_cell_update: X'), or None."""
+    p = os.path.join(ROOT, "profiles", "yee_update_dipole_ellipsoids.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_cell_update:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def write_case(directory, deck, ext, bulk):
+    """A deck directory the oracle (or the FDTD-B200 launcher) can run."""
+    from alpineem_b200.deck import deck_text
+    with open(os.path.join(directory, "inputs.txt"), "w") as f:
+        f.write(deck_text(deck))
+    with open(os.path.join(directory, "inputs.txt.b200"), "w") as f:
+        f.write(ext)
+    bulk.tofile(os.path.join(directory, deck["bulk"]))
+
+
+def oracle_sample(n, warm, steps, threads=None):
+    """Time `steps` oracle steps (after `warm` untimed ones) on an n^3
+    instance of the workload; returns (Mcell-updates/s, threads, cells)."""
+    from alpineem_b200 import workloads
+    if not os.path.exists(ORACLE):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    deck, ext, bulk = workloads.dipole_ellipsoids(n=n)
+    with tempfile.TemporaryDirectory() as d:
+        write_case(d, deck, ext, bulk)
+        del bulk
+        threads = threads or os.cpu_count() or 1
+        env = dict(os.environ, ORACLE_MAX_STEPS=str(warm + steps), ORACLE_WARMUP_STEPS=str(warm),
+                   ORACLE_TIMING_FILE=os.path.join(d, "timing.json"), OMP_NUM_THREADS=str(threads),
+                   OMP_PROC_BIND="close", OMP_PLACES="cores")
+        r = subprocess.run([ORACLE, "inputs.txt"], cwd=d, env=env, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("oracle failed: " + r.stdout[-1000:] + r.stderr[-1000:])
+        with open(os.path.join(d, "timing.json")) as f:
+            t = json.load(f)
+    return t["cells"] * t["steps"] / t["seconds"] / 1e6, t["threads"], t["cells"]
+
+
+def reference_arm(args):
+    """The reference's CPU path on this box's host cores: the oracle on a
+    cpu-n^3 sample of the workload, warm-up then --steps timed steps."""
+    rank, _, world = ranks()
+    if rank != 0:
+        return
+    v, threads, cells = oracle_sample(args.cpu_n, args.warmup, args.steps)
+    n = args.cpu_n
+    sample = ("%d^3 instance of the workload (%d cells, 64 ellipsoids, 684 far-field angles, 16-cell CPML), "
+              "%d timed steps after %d warm-up" % (n, cells, args.steps, args.warmup))
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(cells / (v * 1e6) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [n, n, n], "cpml_cells": 16, "ellipsoids": 64,
+                       "far_field_angles": 684, "deck_steps": 4000},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours(args):
+    import torch
+    import alpineem_b200 as ab
+    from alpineem_b200 import workloads
+    from alpineem_b200.deck import deck_text
+
+    rank, local, world = ranks()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    K, W = args.steps, args.warmup
+    t0 = time.time()
+    deck, ext, bulk = workloads.dipole_ellipsoids(n=args.n)
+    t_gen = time.time() - t0
+    tmp = tempfile.mkdtemp(prefix="aem_bench_")
+    t0 = time.time()
+    sim = ab.Simulation(deck_text=deck_text(deck), ext_text=ext, bulk=bulk, outdir=tmp)
+    t_setup = time.time() - t0
+    cells, bytes_step = sim.workload
+
+    # warm-up, then K timed steps; per-phase events bracket every launch
+    sim.run(W)
+    sim.synchronize()
+    sim.profile(True)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = sim.launches
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.run(K)
+        sim.flush()
+        ev1.record(stream)
+        sim.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = sim.launches - launches0
+    prof = sim.profile_read()
+    sim.profile(False)
+    ms_max = max_over_ranks(ms)
+    value = world * cells * K / (ms_max / 1e3) / 1e6
+
+    # roofline of the Yee update (the fused kernel, or the H and E kernels)
+    t_yee = (prof["update_h"][0] + prof["update_e"][0] + prof["yee"][0]) / K / 1e3
+    peak, peak_kind = hbm_peak()
+    achieved = bytes_step / t_yee / 1e9
+    tpc = dram_traffic_per_cell()
+    kname = "k_yee (fused H+E step)" if prof["yee"][1] else "k_update_h + k_update_e (one Yee step)"
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": round(tpc * cells) if tpc else None,
+                "algorithmic_bytes": round(bytes_step), "bytes_per_cell_update": round(bytes_step / cells, 2)}
+    phases = {k: round(v[0] / K, 4) for k, v in prof.items() if v[1]}
+    sim.close()
+    del sim
+
+    e2e = None
+    if not args.no_e2e:
+        # a complete K-step job through the C ABI from host buffers
+        deck_k = dict(deck, steps=K)
+        pinned = torch.empty(bulk.size, dtype=torch.float32, pin_memory=True)
+        pinned.numpy()[:] = bulk.reshape(-1)
+        host_bulk = pinned.numpy()
+        etmp = tempfile.mkdtemp(prefix="aem_e2e_")
+        barrier()
+        t0 = time.perf_counter()
+        job = ab.Simulation(deck_text=deck_text(deck_k), ext_text=ext, bulk=host_bulk, outdir=etmp)
+        for s in range(1, K + 1):
+            job.run(1)
+            job.probe("port_voltage", 0, first=s, n=1)
+        job.write_outputs()
+        t1 = time.perf_counter()
+        h2d, d2h = job.transfer_bytes
+        job.close()
+        wall = max_over_ranks(t1 - t0)
+        e2e = {"value": round(world * cells * K / wall / 1e6, 3), "unit": UNIT,
+               "h2d_bytes_per_step": round(h2d / K), "d2h_bytes_per_step": round(d2h / K),
+               "seconds": round(wall, 3), "steps": K}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, threads, ccells = oracle_sample(args.cpu_n, 1, args.cpu_steps)
+        cpu = {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "oracle (C/OpenMP restatement of the reference loop) on a %d^3 instance of the workload "
+                         "(%d cells, same CPML, ellipsoids, port and 684 far-field angles), %d timed steps after 1 warm-up"
+                         % (args.cpu_n, ccells, args.cpu_steps)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": round(ms_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": cells, "cpml_cells": 16,
+                           "ellipsoids": 64, "far_field_angles": 684, "deck_steps": deck["steps"],
+                           "l2": "no flush: 28 GB of resident fields and tables, far above the 126 MB L2",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": launches, "phases_ms_per_step": phases,
+                "setup_s": round(t_setup, 2), "workload_gen_s": round(t_gen, 2)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.steps < 1 or args.warmup < 3:
+        sys.exit("--steps must be >= 1 and --warmup >= 3")
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()
