@@ -70,6 +70,8 @@ def load_library():
     lib.aem_launch_count.argtypes = [h, ctypes.POINTER(ctypes.c_longlong)]
     lib.aem_workload.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
     lib.aem_flush.argtypes = [h]
+    lib.aem_dft.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                            ctypes.c_void_p, ctypes.c_void_p]
     lib.aem_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]
     lib.aem_transfer_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     _lib = lib
@@ -77,6 +79,24 @@ def load_library():
 
 
 PHASES = ["update_h", "update_e", "ports", "ff_currents", "ff_bin", "taps", "yee", "other"]
+
+
+def dft(x, dt, freqs, stream=0):
+    """Spectrum of a device time series at the given frequencies:
+    sum_m x[m] exp(-i 2 pi f m dt).  `x` is a CUDA float32 tensor, `freqs`
+    a CUDA float64 tensor (Hz); returns a complex128 CUDA tensor.  Runs the
+    library's kernels (aem_dft) on `stream` (default: the current stream)."""
+    import torch
+    lib = load_library()
+    if x.dtype != torch.float32 or not x.is_cuda or freqs.dtype != torch.float64 or not freqs.is_cuda:
+        raise ValueError("x must be a CUDA float32 tensor and freqs a CUDA float64 tensor")
+    x, freqs = x.contiguous(), freqs.contiguous()
+    out = torch.empty(2 * freqs.numel(), dtype=torch.float64, device=x.device)
+    st = stream or torch.cuda.current_stream(x.device).cuda_stream
+    rc = lib.aem_dft(x.data_ptr(), x.numel(), float(dt), freqs.data_ptr(), freqs.numel(), out.data_ptr(), st)
+    if rc != 0:
+        raise AemError(lib.aem_last_error(None).decode())
+    return torch.view_as_complex(out.view(-1, 2))
 
 
 def check_deck(deck_text, ext_text=None, kmax=False):

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "../../include/alpineem_b200.h"
+#include "aem_dft.h"
 #include "aem_solver.h"
 
 struct aem_handle {
@@ -41,6 +42,11 @@ int guarded(aem_handle* h, F&& f) {
     }
 }
 }  // namespace
+
+namespace aem {
+// error text for entry points that have no handle (aem_last_error(NULL))
+void set_global_error(const std::string& msg) { g_create_err = msg; }
+}  // namespace aem
 
 extern "C" {
 
@@ -237,6 +243,26 @@ int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step) {
     if (!h) return AEM_ERR_ARG;
     if (cells) *cells = h->s->cell_count();
     if (bytes_per_step) *bytes_per_step = h->s->algorithmic_bytes_per_step();
+    return AEM_OK;
+}
+
+int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream) {
+    if (!x || !freqs || !out || n < 1 || nf < 1 || !(dt > 0.0)) return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int chunks = aem::dft_chunks(n, nf);
+    double* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&scratch, sizeof(double) * 2 * (size_t)chunks * nf, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, AEM_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    }
+    e = aem::dft_launch(x, n, dt, freqs, nf, out, scratch, chunks, s);
+    cudaError_t e2 = cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, AEM_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    }
     return AEM_OK;
 }
 

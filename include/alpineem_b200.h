@@ -121,6 +121,17 @@ int aem_transfer_bytes(aem_handle* h, long long* h2d, long long* d2h);
  * 8 CPML psi values per cell of each CPML slab. */
 int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step);
 
+/* Spectrum of a time series at arbitrary frequencies, on the GPU:
+ *   out[2k] + i out[2k+1] = sum_{m<n} x[m] exp(-i 2 pi freqs[k] m dt).
+ * x (n floats), freqs (nf doubles, Hz) and out (2*nf doubles) are device
+ * pointers; the work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without waiting.  Replaces the
+ * numpy FFT of the zero-padded series in utility_scripts/post_processor.py
+ * (:160-215), whose bin k is this sum at k/((padding+1) n dt).  Accumulates
+ * in FP64 in a fixed order (deterministic); takes a temporary device buffer
+ * of 16 * chunks * nf bytes (chunks <= 64) from the stream-ordered pool. */
+int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream);
+
 /* Steps done so far and the deck's step count. */
 int aem_steps(aem_handle* h, int* done, int* total);
 
