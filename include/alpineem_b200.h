@@ -132,6 +132,20 @@ int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step);
  * of 16 * chunks * nf bytes (chunks <= 64) from the stream-ordered pool. */
 int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream);
 
+/* aem_dft for callers that cannot allocate device memory (an application
+ * that keeps all GPU memory in its own arena, a plugin host that forbids
+ * allocation in its callbacks, a real-time loop that must not block on an
+ * allocator).  Same arguments and the same results, bit for bit; it calls
+ * no allocator.  The chunk sums live in one static device array of 1 MiB,
+ * present on every GPU that loads the library until the process exits,
+ * which bounds nf to 65536 frequencies: larger nf fails with AEM_ERR_ARG.
+ * The first call on each device looks up that array's device address (with
+ * the device current); make that first call before any stream capture.
+ * All calls share the array: calls that may overlap on the GPU (different
+ * streams, or different threads) race and must be serialised by the
+ * caller.  This entry point has no counterpart in the reference. */
+int aem_dft_static(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream);
+
 /* Steps done so far and the deck's step count. */
 int aem_steps(aem_handle* h, int* done, int* total);
 
