@@ -312,40 +312,119 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
 // cell c at step n to angle g is the reference's (ref :7667-7730)
 //   t = n + 1/2 + tf(c,g) - 1 (U, from M)   or   n + tf(c,g) - 1 (W, from J),
 //   U(ii) += (1-w) fac dM,  U(ii+1) += w fac dM,  ii = int(t), w = t - ii,
-// with tf(c,g) fixed over the run.  The differences of F.tb steps are kept
-// (F.dbuf) and binned here in one pass: a CTA takes one 32x32 tile of one face
-// and F.group virtual angles (angle, image pass); lane t of each warp owns
-// step n0+t and holds the differences of 16 cells of one tile row in
-// registers.  For every angle the lane walks its 16 cells, summing the two
-// interpolation weights in registers while the bin stays the same and adding
-// the sums into a shared histogram when it changes (lanes own distinct bins,
-// so the shared atomics never collide within an instruction).  Each histogram
+// with tf(c,g) = K0 + Ku*u + Kv*v fixed over the run ((u, v): the face's cell
+// indices; host-precomputed per angle and face).  The differences of F.tb
+// steps are kept (F.dbuf) and binned here in one pass.  A CTA takes one
+// 32x32 tile of one face and a group of virtual angles (angle, image pass)
+// whose delay changes more slowly along one face axis ("walk axis"; the host
+// groups the angles of each face by it).  Lane t of each warp owns step
+// n0+t and holds the differences of an 8-cell strip along the walk axis in
+// registers.  For every angle the lane walks the strip in the direction of
+// increasing delay, summing the two interpolation weights in registers while
+// the bin stays the same; when the bin advances by one, the finished low bin
+// goes to a shared histogram and the high-bin sum carries over as the next
+// run's low-bin sum (both weights of the same bin).  Lanes own distinct bins,
+// so the shared atomics never collide within an instruction.  Each histogram
 // goes to U/W once per batch, one global atomic per non-zero bin, scaled by
-// fac and the image-pass sign.  tf(c,g) = K0 + Ku*u + Kv*v over the face's
-// (u, v) cell indices (host-precomputed per angle and face).
-__global__ void __launch_bounds__(256, 1) k_ff_bin_batch(const __grid_constant__ AemParams P,
+// fac and the image-pass sign.
+constexpr int FF_STRIP = 8;
+// one lane's walk over a strip for one angle, in increasing delay (REV:
+// from the strip's end); see k_ff_bin_batch
+template <bool REV>
+__device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw, float tf0, int w0, float fn, float fnh,
+                                        float* hist, int oU1, int oU2, int oW1, int oW2, int lo_ok, int hi_ok,
+                                        int& bad) {
+    int kU = INT_MIN, kW = INT_MIN;
+    float u1l = 0.0f, u1h = 0.0f, u2l = 0.0f, u2h = 0.0f, w1l = 0.0f, w1h = 0.0f, w2l = 0.0f, w2h = 0.0f;
+#pragma unroll
+    for (int jj = 0; jj < FF_STRIP; jj++) {
+        const int j = REV ? FF_STRIP - 1 - jj : jj;
+        const float tf = fmaf(kw, (float)(w0 + j), tf0);
+        const float tu = (fnh + tf) - 1.0f;
+        const int iu = (int)tu;
+        const float wu = tu - (float)iu;
+        const float tw = (fn + tf) - 1.0f;
+        const int iw = (int)tw;
+        const float ww = tw - (float)iw;
+        if (iu != kU) {
+            if (kU != INT_MIN) {
+                if (kU >= lo_ok && kU <= hi_ok) {
+                    atomicAdd(&hist[oU1 + kU - 1], u1l);
+                    atomicAdd(&hist[oU2 + kU - 1], u2l);
+                    if (iu == kU + 1) {  // the high bin continues as the next low bin
+                        u1l = u1h; u2l = u2h;
+                    } else {
+                        atomicAdd(&hist[oU1 + kU], u1h);
+                        atomicAdd(&hist[oU2 + kU], u2h);
+                        u1l = u2l = 0.0f;
+                    }
+                } else {
+                    bad++;
+                    u1l = u2l = 0.0f;
+                }
+            }
+            kU = iu; u1h = u2h = 0.0f;
+        }
+        if (iw != kW) {
+            if (kW != INT_MIN) {
+                if (kW >= lo_ok && kW <= hi_ok) {
+                    atomicAdd(&hist[oW1 + kW - 1], w1l);
+                    atomicAdd(&hist[oW2 + kW - 1], w2l);
+                    if (iw == kW + 1) {
+                        w1l = w1h; w2l = w2h;
+                    } else {
+                        atomicAdd(&hist[oW1 + kW], w1h);
+                        atomicAdd(&hist[oW2 + kW], w2h);
+                        w1l = w2l = 0.0f;
+                    }
+                } else {
+                    bad++;
+                    w1l = w2l = 0.0f;
+                }
+            }
+            kW = iw; w1h = w2h = 0.0f;
+        }
+        u1l = fmaf(1.0f - wu, d[j][0], u1l); u1h = fmaf(wu, d[j][0], u1h);
+        u2l = fmaf(1.0f - wu, d[j][1], u2l); u2h = fmaf(wu, d[j][1], u2h);
+        w1l = fmaf(1.0f - ww, d[j][2], w1l); w1h = fmaf(ww, d[j][2], w1h);
+        w2l = fmaf(1.0f - ww, d[j][3], w2l); w2h = fmaf(ww, d[j][3], w2h);
+    }
+    if (kU >= lo_ok && kU <= hi_ok) {
+        atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
+        atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
+    } else bad++;
+    if (kW >= lo_ok && kW <= hi_ok) {
+        atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
+        atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
+    } else bad++;
+}
+
+__global__ void __launch_bounds__(256, 2) k_ff_bin_batch(const __grid_constant__ AemParams P,
                                                          const __grid_constant__ FarFieldDev F, int n0, int nt) {
     extern __shared__ float hist[];  // [group][4][hspan]: U1, U2, W1, W2
     __shared__ float ksh[64][3];
-    __shared__ int bsh[64];
+    __shared__ int bsh[64], vash[64];
     const int G = F.group, HS = F.hspan;
     // face (a, s) of this tile
     const long long tile = blockIdx.x;
     int f = 0;
     while (f < 5 && tile >= F.tile0[f + 1]) f++;
+    const int* grp = F.grp + ((long long)f * F.ngrp + blockIdx.y) * 3;
+    const int walk_v = grp[0], first = grp[1], ng = grp[2];
+    if (ng == 0) return;  // uniform over the CTA
     const int a = f >> 1, s = f & 1;
     const long long tl = tile - F.tile0[f];
     const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
     const int nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
     const int u0 = (int)(tl % F.tiles_u[a]) * FF_TILE, v0 = (int)(tl / F.tiles_u[a]) * FF_TILE;
-    const int va0 = blockIdx.y * G;
-    const int ng = min(G, F.nvang - va0);
     const long long n = F.face_n[a];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     for (int e = tid; e < G * 4 * HS; e += blockDim.x) hist[e] = 0.0f;
     if (tid < ng) {
-        const float* k = F.kf + (((long long)(va0 + tid) * 3 + a) * 2 + s) * 3;
+        const int va = F.alist[(long long)f * F.nvang + first + tid];
+        vash[tid] = va;
+        const float* k = F.kf + (((long long)va * 3 + a) * 2 + s) * 3;
         ksh[tid][0] = k[0]; ksh[tid][1] = k[1]; ksh[tid][2] = k[2];
         // lowest bin any contribution of the tile can reach, less a margin
         const float tmin = k[0] + k[1] * (float)(k[1] < 0.0f ? u0 + FF_TILE - 1 : u0) +
@@ -358,65 +437,34 @@ __global__ void __launch_bounds__(256, 1) k_ff_bin_batch(const __grid_constant__
     const bool live = lane < nt;
     const float* dif = reinterpret_cast<const float*>(F.dbuf[a][s]);
     int bad = 0;
-    for (int sub = 0; sub < FF_TILE / 4; sub++) {
-        const int v = v0 + 4 * sub + (warp >> 1);
-        const int ub0 = u0 + 16 * (warp & 1);
-        if (v >= nc || ub0 >= nb) continue;  // warp-uniform
-        float d[16][4];
+    constexpr int STRIPS = FF_TILE * (FF_TILE / FF_STRIP);  // 128 strips per tile
+    for (int sid = warp; sid < STRIPS; sid += 8) {
+        // strip start (u, v) and step along the walk axis
+        const int across = sid / (FF_TILE / FF_STRIP), along = (sid % (FF_TILE / FF_STRIP)) * FF_STRIP;
+        const int us = walk_v ? u0 + across : u0 + along;
+        const int vs = walk_v ? v0 + along : v0 + across;
+        if (us >= nb || vs >= nc) continue;  // warp-uniform
+        float d[FF_STRIP][4];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const bool ok = live && ub0 + j < nb;
-            const long long q = (long long)v * nb + ub0 + j;
+        for (int j = 0; j < FF_STRIP; j++) {
+            const int u = walk_v ? us : us + j, v = walk_v ? vs + j : vs;
+            const bool ok = live && u < nb && v < nc;
+            const long long q = (long long)v * nb + u;
 #pragma unroll
             for (int m = 0; m < 4; m++) d[j][m] = ok ? __ldg(dif + ((long long)m * F.tb + lane) * n + q) : 0.0f;
         }
         for (int g = 0; g < ng; g++) {
-            const float tf0 = fmaf(ksh[g][2], (float)v, ksh[g][0]), ku = ksh[g][1];
+            const float K0 = ksh[g][0], Ku = ksh[g][1], Kv = ksh[g][2];
+            const float kw = walk_v ? Kv : Ku;
+            const float tf0 = walk_v ? fmaf(Ku, (float)us, K0) : fmaf(Kv, (float)vs, K0);
+            const int w0 = walk_v ? vs : us;
             // histogram offsets: bin k of component m of angle g is hist[(4g+m)HS + k - bsh[g]]
             const int oU1 = g * 4 * HS - bsh[g], oU2 = oU1 + HS, oW1 = oU1 + 2 * HS, oW2 = oU1 + 3 * HS;
-            int kU = INT_MIN, kW = INT_MIN;
-            float u1l = 0.0f, u1h = 0.0f, u2l = 0.0f, u2h = 0.0f, w1l = 0.0f, w1h = 0.0f, w2l = 0.0f, w2h = 0.0f;
-            const int lo_ok = bsh[g], hi_ok = bsh[g] + HS - 1;
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const float tf = fmaf(ku, (float)(ub0 + j), tf0);
-                const float tu = (fnh + tf) - 1.0f;
-                const int iu = (int)tu;
-                const float wu = tu - (float)iu;
-                const float tw = (fn + tf) - 1.0f;
-                const int iw = (int)tw;
-                const float ww = tw - (float)iw;
-                if (iu != kU) {
-                    if (kU != INT_MIN) {
-                        if (kU - 1 >= lo_ok && kU <= hi_ok) {
-                            atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
-                            atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
-                        } else bad++;
-                    }
-                    kU = iu; u1l = u1h = u2l = u2h = 0.0f;
-                }
-                if (iw != kW) {
-                    if (kW != INT_MIN) {
-                        if (kW - 1 >= lo_ok && kW <= hi_ok) {
-                            atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
-                            atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
-                        } else bad++;
-                    }
-                    kW = iw; w1l = w1h = w2l = w2h = 0.0f;
-                }
-                u1l = fmaf(1.0f - wu, d[j][0], u1l); u1h = fmaf(wu, d[j][0], u1h);
-                u2l = fmaf(1.0f - wu, d[j][1], u2l); u2h = fmaf(wu, d[j][1], u2h);
-                w1l = fmaf(1.0f - ww, d[j][2], w1l); w1h = fmaf(ww, d[j][2], w1h);
-                w2l = fmaf(1.0f - ww, d[j][3], w2l); w2h = fmaf(ww, d[j][3], w2h);
-            }
-            if (kU - 1 >= lo_ok && kU <= hi_ok) {
-                atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
-                atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
-            } else bad++;
-            if (kW - 1 >= lo_ok && kW <= hi_ok) {
-                atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
-                atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
-            } else bad++;
+            const int lo_ok = bsh[g] + 1, hi_ok = bsh[g] + HS - 1;
+            if (kw >= 0.0f)
+                ff_walk<false>(d, kw, tf0, w0, fn, fnh, hist, oU1, oU2, oW1, oW2, lo_ok, hi_ok, bad);
+            else
+                ff_walk<true>(d, kw, tf0, w0, fn, fnh, hist, oU1, oU2, oW1, oW2, lo_ok, hi_ok, bad);
         }
     }
     if (bad) atomicAdd(F.err, bad);
@@ -429,7 +477,7 @@ __global__ void __launch_bounds__(256, 1) k_ff_bin_batch(const __grid_constant__
         const float h = hist[e];
         if (h == 0.0f) continue;
         const int g = e / (4 * HS), m = (e / HS) & 3, k = e % HS;
-        const int va = va0 + g, ang = va % F.nang, pass = va / F.nang;
+        const int va = vash[g], ang = va % F.nang, pass = va / F.nang;
         const long long gi = (long long)bsh[g] + k;
         if (gi < 0 || gi >= F.len) { atomicAdd(F.err, 1); continue; }
         float sg = 1.0f;
@@ -564,7 +612,7 @@ int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStr
 size_t ff_batch_smem(const FarFieldDev& F) { return (size_t)F.group * 4 * F.hspan * sizeof(float); }
 int launch_ff_bin_batch(const AemParams& P, const FarFieldDev& F, int n0, int nt, cudaStream_t s) {
     if (!F.nang || nt <= 0 || F.tile0[6] == 0) return 0;
-    dim3 grid((unsigned)F.tile0[6], (unsigned)((F.nvang + F.group - 1) / F.group));
+    dim3 grid((unsigned)F.tile0[6], (unsigned)F.ngrp);
     k_ff_bin_batch<<<grid, 256, ff_batch_smem(F), s>>>(P, F, n0, nt);
     return 1;
 }

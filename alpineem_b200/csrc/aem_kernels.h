@@ -55,6 +55,9 @@ struct FarFieldDev {
     int tiles_u[3], tiles_v[3]; // 32x32 tiles per face of each normal
     long long tile0[7];         // first tile of face (a, s) at index 2a+s
     const float* kf;            // [nvang][3][2][3]: K0, Ku, Kv of the retarded-time offset tf(u, v)
+    const int* alist;           // [6 faces][nvang]: virtual angles, those walked along u first
+    const int* grp;             // [6 faces][ngrp][3]: walk along v?, first alist entry, count (0 = none)
+    int ngrp;                   // angle groups per face (grid y of the batch kernel)
     int* err;                   // count of contributions that fell outside a histogram (must stay 0)
 };
 

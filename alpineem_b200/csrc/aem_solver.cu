@@ -464,6 +464,33 @@ void Solver::setup_farfield() {
     F.group = (int)std::min<size_t>(64, smem_max / ((size_t)4 * F.hspan * sizeof(float)));
     F.tb = (!d.kmax && F.group >= 1) ? FF_TB : 1;
     if (F.tb > 1) {
+        // per face: angles whose delay changes more slowly along u are
+        // walked along u, the others along v; groups of F.group angles
+        std::vector<int> alist((size_t)6 * F.nvang), glist;
+        std::vector<std::vector<int>> groups(6);
+        int ngrp = 1;
+        for (int f = 0; f < 6; f++) {
+            const int a = f >> 1, s = f & 1;
+            std::vector<int> cu, cv;
+            for (int va = 0; va < F.nvang; va++) {
+                const float* k = &kf[(((size_t)va * 3 + a) * 2 + s) * 3];
+                (std::fabs(k[1]) <= std::fabs(k[2]) ? cu : cv).push_back(va);
+            }
+            size_t pos = (size_t)f * F.nvang;
+            for (int va : cu) alist[pos++] = va;
+            for (int va : cv) alist[pos++] = va;
+            for (size_t g = 0; g < cu.size(); g += F.group)
+                groups[f].insert(groups[f].end(), {0, (int)g, (int)std::min<size_t>(F.group, cu.size() - g)});
+            for (size_t g = 0; g < cv.size(); g += F.group)
+                groups[f].insert(groups[f].end(), {1, (int)(cu.size() + g), (int)std::min<size_t>(F.group, cv.size() - g)});
+            ngrp = std::max(ngrp, (int)groups[f].size() / 3);
+        }
+        glist.assign((size_t)6 * ngrp * 3, 0);
+        for (int f = 0; f < 6; f++)
+            std::copy(groups[f].begin(), groups[f].end(), glist.begin() + (size_t)f * ngrp * 3);
+        F.ngrp = ngrp;
+        F.alist = (const int*)upload(alist);
+        F.grp = (const int*)upload(glist);
         F.kf = (const float*)upload(kf);
         F.tile0[0] = 0;
         for (int f = 0; f < 6; f++) F.tile0[f + 1] = F.tile0[f] + (long long)F.tiles_u[f >> 1] * F.tiles_v[f >> 1];
