@@ -95,6 +95,7 @@ void ff_batch_prepare();                     // raise the kernel's shared-memory
 // sheets, Drude poles, gridded ports, kmax
 bool yee_fused_ok(const AemParams& P, int gridded_ports);
 int launch_yee(const AemParams& P, cudaStream_t s);
+int launch_yee4(const AemParams& P, cudaStream_t s);  // aem_yee4.cu (no x/y periodicity)
 int launch_taps(const AemParams& P, const TapDev& T, const FarFieldDev& F, int counter, int steps, cudaStream_t s);
 
 }  // namespace aem

@@ -404,10 +404,12 @@ void Solver::setup_farfield() {
         int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
         F.fac[a] = dl[b] * dl[c] / (4.0f * pi * d.del_t * c0);
         F.has[a] = !d.pbc[a];
-        // an inverted box (grid smaller than PML + TF/SF buffer) has empty
-        // faces, as the reference's loops over it are empty
+        // a face whose tangential range is inverted (grid smaller than PML +
+        // buffer along that axis) is empty, as the reference's loops over it
+        // are; an inverted range along the normal still has its two planes
+        // (the reference visits ff_low and ff_high whatever their order)
         const long long nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
-        F.face_n[a] = (F.has[a] && nb > 0 && nc > 0 && F.hi[a] >= F.lo[a]) ? nb * nc : 0;
+        F.face_n[a] = (F.has[a] && nb > 0 && nc > 0) ? nb * nc : 0;
         F.tiles_u[a] = F.face_n[a] ? (int)((nb + FF_TILE - 1) / FF_TILE) : 0;
         F.tiles_v[a] = F.face_n[a] ? (int)((nc + FF_TILE - 1) / FF_TILE) : 0;
     }
@@ -462,7 +464,8 @@ void Solver::setup_farfield() {
     F.hspan = (int)std::ceil(span) + FF_TB + 8;
     const size_t smem_max = 96 * 1024;
     F.group = (int)std::min<size_t>(64, smem_max / ((size_t)4 * F.hspan * sizeof(float)));
-    F.tb = (!d.kmax && F.group >= 1) ? FF_TB : 1;
+    // (AEM_FF_PER_STEP=1 keeps the per-step binning kernel, for A/B checks)
+    F.tb = (!d.kmax && F.group >= 1 && !getenv_flag("AEM_FF_PER_STEP")) ? FF_TB : 1;
     if (F.tb > 1) {
         // per face: angles whose delay changes more slowly along u are
         // walked along u, the others along v; groups of F.group angles

@@ -584,7 +584,16 @@ static bool yee_pipe_disabled() {
     return off;
 }
 
+static bool env_flag(const char* name) {
+    const char* v = std::getenv(name);
+    return v && *v && std::strcmp(v, "0") != 0;
+}
+
 int launch_yee(const AemParams& P, cudaStream_t s) {
+    // grids without x/y periodicity: the 4-cells-per-thread kernel
+    // (AEM_YEE_PIPE=1 selects the scalar staged kernel instead)
+    static const bool pipe = env_flag("AEM_YEE_PIPE");
+    if (!P.per[0] && !P.per[1] && !yee_pipe_disabled() && !pipe) return launch_yee4(P, s);
     if (!P.per[0] && !P.per[1] && !yee_pipe_disabled()) {
         // the shared-memory limit is a per-device property of the function
         static bool attr_set[64] = {};

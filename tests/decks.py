@@ -89,6 +89,15 @@ DECKS = {
                          objects=[("block", 4, (20, 18, 60), (1, 1, 6)), ("block", 4, (20, 18, 67), (1, 1, 6)),
                                   ("cylinder", 6, "z", (20, 18, 100), (40, 3))],
                          ports=[("basic", "z", 50, (20, 18, 66), (1, 1, 1))]),
+    # long in x: three 128-cell tiles of the vectorised fused kernel, so the
+    # -x halo column between CTAs is recomputed; materials across the tile
+    # seams at x = 128 and 256, far field on all faces
+    "fused_long_x": dict(n=(300, 22, 26), steps=220, f="15E9", pulse=1, excitation=("antenna", 1, 0, 1),
+                         ff=[(90, 0), (45, 120)], ffc=(150, 11, 13),
+                         mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (4, 3, 2), (0.01, 0, 0))],
+                         objects=[("block", 4, (150, 11, 8), (1, 1, 4)), ("block", 4, (150, 11, 14), (1, 1, 4)),
+                                  ("block", 5, (120, 6, 6), (20, 8, 12)), ("sphere", 5, (256, 11, 13), 5)],
+                         ports=[("basic", "z", 50, (150, 11, 13), (1, 1, 1))]),
     # the throughput workload at 48^3: bulk-file ellipsoids, 6-cell CPML
     # (sidecar), a 1-cell port and 56 far-field angles
     "ellipsoids_small": "ellipsoids_small",
