@@ -29,16 +29,19 @@
 
 namespace aem {
 
-constexpr int Y4_TX = 128, Y4_TY = 8, Y4_ZC = 64, Y4_SLOTS = 4;
+constexpr int Y4_TX = 128, Y4_TY = 8, Y4_ZC = 64;
 constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;  // E tile 136 x 10, x from x0-4
 constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;  // H tile 132 x 9, x from x0-4
 constexpr int Y4_IW = Y4_TX + 16;                    // ids 144 bytes x 9 rows, x from x0-16
-constexpr int Y4_SLOT_F = 3 * Y4_ER * Y4_EW + 3 * Y4_HR * Y4_HW;
-constexpr int Y4_SLOT_B = Y4_SLOT_F * 4 + Y4_HR * Y4_IW;
+// three rings: E planes k, k+1, k+2; H planes k, k+1; id planes k-1, k, k+1
+constexpr int Y4_ES = 3, Y4_HS = 2, Y4_IS = 3;
+constexpr int Y4_E_B = 3 * Y4_ER * Y4_EW * 4, Y4_H_B = 3 * Y4_HR * Y4_HW * 4, Y4_I_B = Y4_HR * Y4_IW;
 constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+7
 constexpr int Y4_NMAT = AEM_MAX_MATERIALS;
-constexpr size_t Y4_SMEM = (size_t)Y4_SLOTS * Y4_SLOT_B + (size_t)Y4_HN_F * 4 + (size_t)Y4_NMAT * 6 * 4;
-static_assert(Y4_SLOT_B % 16 == 0, "slots must stay 16-byte aligned");
+constexpr size_t Y4_OFF_H = (size_t)Y4_ES * Y4_E_B, Y4_OFF_I = Y4_OFF_H + (size_t)Y4_HS * Y4_H_B;
+constexpr size_t Y4_OFF_HN = Y4_OFF_I + (size_t)Y4_IS * Y4_I_B;
+constexpr size_t Y4_SMEM = Y4_OFF_HN + (size_t)Y4_HN_F * 4 + (size_t)Y4_NMAT * 6 * 4;
+static_assert(Y4_E_B % 16 == 0 && Y4_H_B % 16 == 0 && Y4_I_B % 16 == 0, "tiles must stay 16-byte aligned");
 
 __device__ inline float ldf4(const void* b, long long i) { return reinterpret_cast<const float*>(b)[i]; }
 __device__ inline void stf4(void* b, long long i, float v) { reinterpret_cast<float*>(b)[i] = v; }
@@ -58,14 +61,12 @@ __device__ inline float psi4(const void* rd, void* wr, bool store, float b, floa
     return nw;
 }
 
-// request plane p (wrapped; -1 / SZ = absent) into ring slot `slot`
-__device__ inline void y4_issue(const AemParams& P, unsigned char* smem, int slot, int p, int x0, int y0) {
-    float* E = reinterpret_cast<float*>(smem + (size_t)slot * Y4_SLOT_B);
-    float* H = E + 3 * Y4_ER * Y4_EW;
-    unsigned char* I = smem + (size_t)slot * Y4_SLOT_B + Y4_SLOT_F * 4;
+// request the tiles of plane p (wrapped; -1 / SZ = absent): E into `E`,
+// H into `H`, ids into `I` (a null destination skips that tile)
+__device__ inline void y4_issue(const AemParams& P, float* E, float* H, unsigned char* I, int p, int x0, int y0) {
     const bool pv = p >= 0 && p < P.SZ;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    constexpr int nE = 3 * Y4_ER * (Y4_EW / 4), nH = 3 * Y4_HR * (Y4_HW / 4), nI = Y4_HR * (Y4_IW / 16);
+    const int nE = E ? 3 * Y4_ER * (Y4_EW / 4) : 0, nH = H ? 3 * Y4_HR * (Y4_HW / 4) : 0, nI = I ? Y4_HR * (Y4_IW / 16) : 0;
     const long long pbase = pv ? (long long)p * P.plane : 0;
     for (int q = tid; q < nE + nH + nI; q += nt) {
         if (q < nE) {
@@ -93,19 +94,19 @@ __device__ inline void y4_issue(const AemParams& P, unsigned char* smem, int slo
 }
 
 // H_new of one cell (k_update_h's expressions; psi from psi_h, to psi_h2 when store)
-__device__ inline void y4_h_cell(const AemParams& P, int px, int py, int pz, float ex, float ey, float ez, float ex_jp,
-                                 float ez_jp, float ey_ip, float ez_ip, float ex_kp, float ey_kp, float hx0, float hy0,
-                                 float hz0, bool store, float& hxv, float& hyv, float& hzv) {
+__device__ __noinline__ float3 y4_h_cell(const AemParams& P, int px, int py, int pz, float ex, float ey, float ez,
+                                          float ex_jp, float ez_jp, float ey_ip, float ez_ip, float ex_kp, float ey_kp,
+                                          float hx0, float hy0, float hz0, bool store) {
     const int i = px + 1, j = py + 1, k = pz + 1;
     const float DB = P.DB;
     const float dhx = P.den_h[0][i - 1], dhy = P.den_h[1][j - 1], dhz = P.den_h[2][k - 1];
-    hxv = hx0 + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
-    hyv = hy0 + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
-    hzv = hz0 + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
+    float hxv = hx0 + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
+    float hyv = hy0 + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
+    float hzv = hz0 + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
     const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
     const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
     const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-    if (!(qx_lo | qx_hi | qy_lo | qy_hi | qz_lo | qz_hi)) return;
+    if (!(qx_lo | qx_hi | qy_lo | qy_hi | qz_lo | qz_hi)) return make_float3(hxv, hyv, hzv);
     if (qy_lo) hxv = hxv + DB * psi4(P.psi_h[0][1][0], P.psi_h2[0][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
     if (qy_hi) hxv = hxv + DB * psi4(P.psi_h[0][1][1], P.psi_h2[0][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
     if (qz_lo) hxv = hxv + DB * psi4(P.psi_h[0][2][0], P.psi_h2[0][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
@@ -118,9 +119,52 @@ __device__ inline void y4_h_cell(const AemParams& P, int px, int py, int pz, flo
     if (qx_hi) hzv = hzv + DB * psi4(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
     if (qy_lo) hzv = hzv + DB * psi4(P.psi_h[2][1][0], P.psi_h2[2][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
     if (qy_hi) hzv = hzv + DB * psi4(P.psi_h[2][1][1], P.psi_h2[2][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+    return make_float3(hxv, hyv, hzv);
 }
 
 // Ga/Gb of an E edge from its four cell ids (reference order, ref :2516-2527)
+// CPML terms of one H cell added to bulk values (the k_update_h order:
+// Hx y then z, Hy x then z, Hz x then y)
+__device__ __noinline__ float3 y4_h_pml(const AemParams& P, int px, int py, int pz, float dzy, float dyz, float dzx,
+                                        float dxz, float dyx, float dxy, bool store, float hxv, float hyv, float hzv) {
+    // dzy = ez - ez_jp, dyz = ey_kp - ey, dzx = ez_ip - ez, dxz = ex - ex_kp, dyx = ey - ey_ip, dxy = ex_jp - ex
+    const int i = px + 1, j = py + 1, k = pz + 1;
+    const float DB = P.DB;
+    const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
+    const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+    const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
+    if (qy_lo) hxv = hxv + DB * psi4(P.psi_h[0][1][0], P.psi_h2[0][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], dzy, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+    if (qy_hi) hxv = hxv + DB * psi4(P.psi_h[0][1][1], P.psi_h2[0][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], dzy, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+    if (qz_lo) hxv = hxv + DB * psi4(P.psi_h[0][2][0], P.psi_h2[0][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], dyz, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+    if (qz_hi) hxv = hxv + DB * psi4(P.psi_h[0][2][1], P.psi_h2[0][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], dyz, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+    if (qx_lo) hyv = hyv + DB * psi4(P.psi_h[1][0][0], P.psi_h2[1][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dzx, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+    if (qx_hi) hyv = hyv + DB * psi4(P.psi_h[1][0][1], P.psi_h2[1][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dzx, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+    if (qz_lo) hyv = hyv + DB * psi4(P.psi_h[1][2][0], P.psi_h2[1][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], dxz, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+    if (qz_hi) hyv = hyv + DB * psi4(P.psi_h[1][2][1], P.psi_h2[1][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], dxz, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+    if (qx_lo) hzv = hzv + DB * psi4(P.psi_h[2][0][0], P.psi_h2[2][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dyx, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+    if (qx_hi) hzv = hzv + DB * psi4(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dyx, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+    if (qy_lo) hzv = hzv + DB * psi4(P.psi_h[2][1][0], P.psi_h2[2][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], dxy, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+    if (qy_hi) hzv = hzv + DB * psi4(P.psi_h[2][1][1], P.psi_h2[2][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], dxy, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+    return make_float3(hxv, hyv, hzv);
+}
+
+// CPML terms of one E cell and component added to its bulk value
+__device__ __noinline__ float y4_e_pml(const AemParams& P, int comp, int px, int py, int pz, float e, float gb, float d1,
+                                       float d2) {
+    const int i = px + 1, j = py + 1, k = pz + 1;
+    const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
+    const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
+    const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
+    const int a1 = comp == 0 ? 1 : 0, a2 = comp == 2 ? 1 : 2;
+    const int q1l = a1 == 0 ? qxl : qyl, q1h = a1 == 0 ? qxh : qyh;
+    const int q2l = a2 == 1 ? qyl : qzl, q2h = a2 == 1 ? qyh : qzh;
+    if (q1l) e = e + gb * psi4(P.psi_e[comp][a1][0], P.psi_e[comp][a1][0], true, P.be[a1][0][q1l - 1], P.ce[a1][0][q1l - 1], d1, P.del[a1], psi_idx(P, a1, q1l, px, py, pz, P.npml[a1][0]));
+    if (q1h) e = e + gb * psi4(P.psi_e[comp][a1][1], P.psi_e[comp][a1][1], true, P.be[a1][1][q1h - 1], P.ce[a1][1][q1h - 1], d1, P.del[a1], psi_idx(P, a1, q1h, px, py, pz, P.npml[a1][1]));
+    if (q2l) e = e + gb * psi4(P.psi_e[comp][a2][0], P.psi_e[comp][a2][0], true, P.be[a2][0][q2l - 1], P.ce[a2][0][q2l - 1], d2, P.del[a2], psi_idx(P, a2, q2l, px, py, pz, P.npml[a2][0]));
+    if (q2h) e = e + gb * psi4(P.psi_e[comp][a2][1], P.psi_e[comp][a2][1], true, P.be[a2][1][q2h - 1], P.ce[a2][1][q2h - 1], d2, P.del[a2], psi_idx(P, a2, q2h, px, py, pz, P.npml[a2][1]));
+    return e;
+}
+
 __device__ inline void y4_gagb(const AemParams& P, const float* gab, int c, int i0, int i1, int i2, int i3, float& ga,
                                float& gb) {
     if (i0 == i1 && i0 == i2 && i0 == i3) {
@@ -161,7 +205,7 @@ __device__ inline void y4_h_group(const AemParams& P, const float* E0, const flo
     const bool upd_all = xb + 3 <= hxm && py >= 0 && py <= hym && pz <= hzm;
     const bool no_pml = i0 >= P.npml[0][0] && xb + 4 <= P.X - P.npml[0][1] && j >= P.npml[1][0] &&
                         j <= P.Y - P.npml[1][1] && k >= P.npml[2][0] && k <= P.Z - P.npml[2][1];
-    if (upd_all && no_pml) {
+    if (upd_all) {
         const float DB = P.DB, dhy = P.den_h[1][j - 1], dhz = P.den_h[2][k - 1];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
@@ -169,6 +213,15 @@ __device__ inline void y4_h_group(const AemParams& P, const float* E0, const flo
             hx[e] = vhx[e] + DB * ((vez[e] - vezj[e]) * dhy + (veyk[e] - vey[e]) * dhz);
             hy[e] = vhy[e] + DB * ((vezi[e] - vez[e]) * dhx + (vex[e] - vexk[e]) * dhz);
             hz[e] = vhz[e] + DB * ((vey[e] - veyi[e]) * dhx + (vexj[e] - vex[e]) * dhy);
+        }
+        if (!no_pml) {
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+            {
+                const float3 h = y4_h_pml(P, xb + e, py, pz, vez[e] - vezj[e], veyk[e] - vey[e], vezi[e] - vez[e],
+                                          vex[e] - vexk[e], vey[e] - veyi[e], vexj[e] - vex[e], store, hx[e], hy[e], hz[e]);
+                hx[e] = h.x; hy[e] = h.y; hz[e] = h.z;
+            }
         }
         if (store) {
             const long long c = lin(P, xb, py, pz);
@@ -183,8 +236,9 @@ __device__ inline void y4_h_group(const AemParams& P, const float* E0, const flo
         const int px = xb + e;
         hx[e] = vhx[e]; hy[e] = vhy[e]; hz[e] = vhz[e];
         if (px <= hxm && py >= 0 && py <= hym && pz <= hzm) {
-            y4_h_cell(P, px, py, pz, vex[e], vey[e], vez[e], vexj[e], vezj[e], veyi[e], vezi[e], vexk[e], veyk[e], vhx[e],
-                      vhy[e], vhz[e], store, hx[e], hy[e], hz[e]);
+            const float3 h = y4_h_cell(P, px, py, pz, vex[e], vey[e], vez[e], vexj[e], vezj[e], veyi[e], vezi[e], vexk[e],
+                                       veyk[e], vhx[e], vhy[e], vhz[e], store);
+            hx[e] = h.x; hy[e] = h.y; hz[e] = h.z;
             if (store) {
                 const long long c = lin(P, px, py, pz);
                 stf4(P.H2[0], c, hx[e]);
@@ -196,24 +250,24 @@ __device__ inline void y4_h_group(const AemParams& P, const float* E0, const flo
 }
 
 // the -x halo cell (x0-1, py) of a row: Hy, Hz (never stored)
-__device__ inline void y4_h_xhalo(const AemParams& P, const float* E0, const float* E1, const float* Ho, int r, int x0,
-                                  int py, int pz, int hxm, int hym, int hzm, float& hyv, float& hzv) {
+__device__ __noinline__ float2 y4_h_xhalo(const AemParams& P, const float* E0, const float* E1, const float* Ho, int r,
+                                           int x0, int py, int pz, int hxm, int hym, int hzm) {
     const int c3 = 3;  // tile column of x0-1
-    hyv = Ho[(1 * Y4_HR + r) * Y4_HW + c3];
-    hzv = Ho[(2 * Y4_HR + r) * Y4_HW + c3];
+    const float hyv = Ho[(1 * Y4_HR + r) * Y4_HW + c3];
+    const float hzv = Ho[(2 * Y4_HR + r) * Y4_HW + c3];
     const int px = x0 - 1;
-    if (px < 0 || px > hxm || py < 0 || py > hym || pz > hzm) return;
+    if (px < 0 || px > hxm || py < 0 || py > hym || pz > hzm) return make_float2(hyv, hzv);
     const float* Ex = E0 + (0 * Y4_ER + r) * Y4_EW;
     const float* Ey = E0 + (1 * Y4_ER + r) * Y4_EW;
     const float* Ez = E0 + (2 * Y4_ER + r) * Y4_EW;
-    float hx_unused;
-    y4_h_cell(P, px, py, pz, Ex[c3], Ey[c3], Ez[c3], Ex[Y4_EW + c3], Ez[Y4_EW + c3], Ey[c3 + 1], Ez[c3 + 1],
-              E1[(0 * Y4_ER + r) * Y4_EW + c3], E1[(1 * Y4_ER + r) * Y4_EW + c3], Ho[(0 * Y4_HR + r) * Y4_HW + c3], hyv,
-              hzv, false, hx_unused, hyv, hzv);
+    const float3 h = y4_h_cell(P, px, py, pz, Ex[c3], Ey[c3], Ez[c3], Ex[Y4_EW + c3], Ez[Y4_EW + c3], Ey[c3 + 1],
+                               Ez[c3 + 1], E1[(0 * Y4_ER + r) * Y4_EW + c3], E1[(1 * Y4_ER + r) * Y4_EW + c3],
+                               Ho[(0 * Y4_HR + r) * Y4_HW + c3], hyv, hzv, false);
+    return make_float2(h.y, h.z);
 }
 
 // E_new of one cell and one component (k_update_e's expressions)
-__device__ inline float y4_e_comp(const AemParams& P, const float* gab, int comp, int px, int py, int pz, float eold,
+__device__ __noinline__ float y4_e_comp(const AemParams& P, const float* gab, int comp, int px, int py, int pz, float eold,
                                   float d1, float d2, float den1, float den2, int i0, int i1, int i2, int i3) {
     const float curl = d1 * den1 + d2 * den2;
     float ga, gb;
@@ -234,10 +288,10 @@ __device__ inline float y4_e_comp(const AemParams& P, const float* gab, int comp
     return e;
 }
 
-__global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_constant__ AemParams P) {
+__global__ void __maxnreg__(112) k_yee4(const __grid_constant__ AemParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    float* Hn = reinterpret_cast<float*>(smem + (size_t)Y4_SLOTS * Y4_SLOT_B);  // [2][9][128]: hx, hz of H_new(k)
-    float* gab = Hn + Y4_HN_F;                                                 // [mat][6]: ga xyz, gb xyz
+    float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);  // [2][9][128]: hx, hz of H_new(k)
+    float* gab = Hn + Y4_HN_F;                              // [mat][6]: ga xyz, gb xyz
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = lane + 32 * w, nthr = 32 * (Y4_TY + 1);
     const int x0 = blockIdx.x * Y4_TX, y0 = blockIdx.y * Y4_TY;
@@ -249,10 +303,13 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
         gab[q] = c < 3 ? P.ucoef[m].ga[c] : P.ucoef[m].gb[c - 3];
     }
     auto zw = [&](int p) { return P.per[2] ? (p % P.SZ + P.SZ) % P.SZ : p; };
-    auto slot_of = [&](int p) { return ((p % Y4_SLOTS) + Y4_SLOTS) % Y4_SLOTS; };
-    auto Es = [&](int p) { return reinterpret_cast<const float*>(smem + (size_t)slot_of(p) * Y4_SLOT_B); };
-    auto Hs = [&](int p) { return Es(p) + 3 * Y4_ER * Y4_EW; };
-    auto Is = [&](int p) { return smem + (size_t)slot_of(p) * Y4_SLOT_B + Y4_SLOT_F * 4; };
+    auto md = [](int p, int m) { return ((p % m) + m) % m; };
+    auto Ew = [&](int p) { return reinterpret_cast<float*>(smem + (size_t)md(p, Y4_ES) * Y4_E_B); };
+    auto Hw = [&](int p) { return reinterpret_cast<float*>(smem + Y4_OFF_H + (size_t)md(p, Y4_HS) * Y4_H_B); };
+    auto Iw = [&](int p) { return smem + Y4_OFF_I + (size_t)md(p, Y4_IS) * Y4_I_B; };
+    auto Es = [&](int p) { return (const float*)Ew(p); };
+    auto Hs = [&](int p) { return (const float*)Hw(p); };
+    auto Is = [&](int p) { return (const unsigned char*)Iw(p); };
 
     // this thread's cells: tile row r (0 = the -y halo row), x = xb..xb+3
     const int r = w == Y4_TY ? 0 : w + 1;
@@ -261,9 +318,10 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
     const bool own = w < Y4_TY && py < P.SY;
 
     const bool below = P.per[2] || z0 > 0;
-    y4_issue(P, smem, slot_of(z0 - 1), below ? zw(z0 - 1) : -1, x0, y0);
-    y4_issue(P, smem, slot_of(z0), zw(z0), x0, y0);
-    y4_issue(P, smem, slot_of(z0 + 1), zw(z0 + 1), x0, y0);
+    // prologue: E of planes z0-1..z0+1, H and ids of z0-1 and z0
+    y4_issue(P, Ew(z0 - 1), Hw(z0 - 1), Iw(z0 - 1), below ? zw(z0 - 1) : -1, x0, y0);
+    y4_issue(P, Ew(z0), Hw(z0), Iw(z0), zw(z0), x0, y0);
+    y4_issue(P, Ew(z0 + 1), nullptr, nullptr, zw(z0 + 1), x0, y0);
     cp_commit4();
     cp_wait0();
     __syncthreads();
@@ -278,11 +336,13 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
 
     for (int k = z0; k < z1; k++) {
         const int pz = zw(k);
-        // plane k+1 has landed and every thread is done with plane k-1;
-        // plane k+2 goes into the slot of plane k-2
+        // E(k+1), H(k), ids(k) have landed and every thread is done with
+        // plane k-1: E(k+2), H(k+1), ids(k+1) reuse the slots of E(k-1),
+        // H(k-1), ids(k-2)
         cp_wait0();
         __syncthreads();
-        y4_issue(P, smem, slot_of(k + 2), k + 2 <= z1 ? zw(k + 2) : -1, x0, y0);
+        y4_issue(P, Ew(k + 2), nullptr, nullptr, k + 2 <= z1 ? zw(k + 2) : -1, x0, y0);
+        y4_issue(P, nullptr, Hw(k + 1), Iw(k + 1), k + 1 < z1 ? zw(k + 1) : -1, x0, y0);
         cp_commit4();
 
         // ---- H_new(k): own rows, the -y halo row (warp 8), the -x halo cell (lane 0)
@@ -293,7 +353,10 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
         else
             for (int e = 0; e < 4; e++) hx[e] = hy[e] = hz[e] = 0.0f;
         float hy_xh = 0.0f, hz_xh = 0.0f;
-        if (lane == 0 && own) y4_h_xhalo(P, E0, Es(k + 1), Hs(k), r, x0, py, pz, hxm, hym, hzm, hy_xh, hz_xh);
+        if (lane == 0 && own) {
+            const float2 hh = y4_h_xhalo(P, E0, Es(k + 1), Hs(k), r, x0, py, pz, hxm, hym, hzm);
+            hy_xh = hh.x; hz_xh = hh.y;
+        }
         *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
         *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
         __syncthreads();
@@ -330,7 +393,7 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
                 const bool uniform = w_a0 == rep && w_a1 == rep && w_b0 == rep && w_b1 == rep && a0[-1] == m &&
                                      a1[-1] == m && b0[-1] == m;
                 float ex_n[4], ey_n[4], ez_n[4];
-                if (upd_all && no_pml && uniform) {
+                if (upd_all && uniform) {
                     const float gax = gab[m * 6 + 0], gay = gab[m * 6 + 1], gaz = gab[m * 6 + 2];
                     const float gbx = gab[m * 6 + 3], gby = gab[m * 6 + 4], gbz = gab[m * 6 + 5];
 #pragma unroll
@@ -339,6 +402,14 @@ __global__ void __launch_bounds__(32 * (Y4_TY + 1), 1) k_yee4(const __grid_const
                         ex_n[e] = gax * vex[e] + gbx * ((hz[e] - hzj[e]) * dey + (hyp[e] - hy[e]) * dez);
                         ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex + (hx[e] - hxp[e]) * dez);
                         ez_n[e] = gaz * vez[e] + gbz * ((hy[e] - him_y[e]) * dex + (hxj[e] - hx[e]) * dey);
+                    }
+                    if (!no_pml) {
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            ex_n[e] = y4_e_pml(P, 0, xb + e, py, pz, ex_n[e], gbx, hz[e] - hzj[e], hyp[e] - hy[e]);
+                            ey_n[e] = y4_e_pml(P, 1, xb + e, py, pz, ey_n[e], gby, him_z[e] - hz[e], hx[e] - hxp[e]);
+                            ez_n[e] = y4_e_pml(P, 2, xb + e, py, pz, ez_n[e], gbz, hy[e] - him_y[e], hxj[e] - hx[e]);
+                        }
                     }
                     const long long c = lin(P, xb, py, pz);
                     *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[0]) + c) = make_float4(ex_n[0], ex_n[1], ex_n[2], ex_n[3]);
