@@ -52,6 +52,22 @@ __device__ inline int wrap_dn(const AemParams& P, int a, int p, int S, bool* wra
     return p - 1;
 }
 
+// num / dl of the CPML update psi = b psi + c diff / dl (num = c diff),
+// rounded as written.  A zero numerator is returned as it is: +-0 / dl
+// (dl > 0) is that same signed zero, and the IEEE division would otherwise
+// take its slow path for it (the CPML fields are exactly zero until a wave
+// reaches them).  The test is a real branch (a select would still run the
+// division); the division is the one `/` compiles to with -ftz=true.
+__device__ __forceinline__ float cpml_div(float num, float dl) {
+    float q;
+    asm("{\n\t.reg .pred z;\n\tmov.b32 %0, %1;\n\tsetp.eq.f32 z, %1, 0f00000000;\n\t@z bra CPML_DIV_DONE;\n\t"
+        "div.rn.ftz.f32 %0, %1, %2;\n\tCPML_DIV_DONE:\n\t}"
+        : "=f"(q)
+        : "f"(num), "f"(dl));
+    return q;
+}
+__device__ __forceinline__ cf cpml_div(cf num, float dl) { return {cpml_div(num.x, dl), cpml_div(num.y, dl)}; }
+
 __device__ inline long long lin(const AemParams& P, int px, int py, int pz) {
     return ((long long)pz * P.SY + py) * P.PX + px;
 }

@@ -64,6 +64,12 @@ void Solver::finalize_and_write() {
         d2h_bytes_ += sizeof err;
         if (err) throw std::runtime_error("far-field binning: " + std::to_string(err) + " contributions outside their histogram");
     }
+    if (P_.err) {
+        int err = 0;
+        AEM_CUDA(cudaMemcpy(&err, P_.err, sizeof err, cudaMemcpyDeviceToHost));
+        d2h_bytes_ += sizeof err;
+        if (err) throw std::runtime_error("fused field update: " + std::to_string(err) + " tiles gave up waiting for their copies");
+    }
 
     // plane sums, normalised per ref :8342-8361 / :8412-8435
     std::vector<cplx> refl, trans, refl_tm, trans_tm;

@@ -45,7 +45,7 @@ __device__ inline T ld_dn(const AemParams& P, const void* base, long long i, boo
 template <typename T>
 __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T diff, float dl, long long q) {
     T old = ld<T>(psi, q);
-    T nw = b * old + c * diff / dl;
+    T nw = b * old + cpml_div(c * diff, dl);
     st<T>(psi, q, nw);
     return nw;
 }

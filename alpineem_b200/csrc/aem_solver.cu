@@ -109,6 +109,7 @@ void Solver::setup_fused() {
     }
     fused_ = yee_fused_ok(P_, gridded) && !split_ && !getenv_flag("AEM_TWO_KERNEL");
     if (!fused_) return;
+    P_.err = (int*)alloc(sizeof(int));
     for (int c = 0; c < 3; c++) {
         P_.E2[c] = alloc((size_t)m_.cells * es_);
         P_.H2[c] = alloc((size_t)m_.cells * es_);

@@ -124,4 +124,6 @@ struct AemParams {
     void* E2[3];
     void* H2[3];
     void* psi_h2[3][3][2];
+    // device counter of fused-step CTAs that gave up a bounded wait (0 = ok)
+    int* err;
 };

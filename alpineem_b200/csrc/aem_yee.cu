@@ -50,7 +50,7 @@ struct HNb {
 // read from `rd`, written to `wr` when `store`
 __device__ inline float psi_term(const void* rd, void* wr, bool store, float b, float c, float diff, float dl,
                                  long long q) {
-    const float nw = b * ldf(rd, q) + c * diff / dl;
+    const float nw = b * ldf(rd, q) + cpml_div(c * diff, dl);
     if (store) stf(wr, q, nw);
     return nw;
 }

@@ -1,100 +1,178 @@
-// aem_yee4.cu -- fused H+E step, 4 cells per thread (grids without x/y
-// periodicity; any z).
+// aem_yee4.cu -- fused H+E step, 4 cells per thread, tiles fed by TMA
+// (grids without x/y periodicity; any z).
 //
 // Same arithmetic, statement for statement, as k_update_h / k_update_e
 // (bulk curl fdtd_solver.f90:4442-4484 / :5667-5710, CPML :5227-5375 /
-// :6522-6670), so the fields are bit-identical to the other paths.
+// :6522-6670), so the fields are bit-identical to the other paths: every
+// FP32 operation of a cell is the reference's, in its order, rounded to
+// nearest with subnormals flushed.  (Packed .f32x2 arithmetic is not used:
+// the assembler fuses a packed multiply into a following packed add even
+// with .rn and contraction disabled, which changes the rounding.)
 //
-// A CTA owns a 128 x 8 (x, y) column tile and marches a z chunk.  Warps 0..7
-// own rows y0..y0+7; lane l owns the four cells x0+4l .. x0+4l+3, so every
-// shared-memory and global access of a cell group is one 16-byte operation.
-// Warp 8 computes the -y halo row of H (y0-1), which the E update of row y0
-// needs; lane 0 of warps 0..7 computes the -x halo cell (x0-1).  Per plane
-// p, a ring slot receives by cp.async (16-byte chunks, zero-filled off the
-// grid): E_old(p) on rows y0-1..y0+8, x0-4..x0+131; H_old(p) on rows
-// y0-1..y0+7, x0-4..x0+127; the material ids of rows y0-1..y0+7,
-// x0-16..x0+127.  Plane k+2 is requested while plane k is computed.  Fields
-// and H-psi are double-buffered (read E/H/psi_h, write E2/H2/psi_h2), so halo
-// values recomputed here never race with their owners' stores.
+// A CTA owns a 128 x 8 (x, y) column tile and marches a z chunk of 64
+// planes.  Warps 0..7 own rows y0..y0+7; lane l owns the four cells
+// x0+4l .. x0+4l+3, so every shared-memory and global access of a cell
+// group is one 16-byte operation.  Warp 8 computes Hx, Hz of the -y halo
+// row (y0-1), which the E update of row y0 needs; lane 0 of warps 0..7
+// computes Hy, Hz of the -x halo cell (x0-1).
 //
-// Per cell group the fast path covers interior cells outside the CPML whose
-// seven surrounding cells share one material (ga/gb from a shared-memory
-// copy of the material table); every other cell takes the per-cell path
-// with the reference's 4-cell material average and the CPML terms.
+// Per plane p one thread requests by TMA (cp.async.bulk.tensor, zero fill
+// outside the grid) E_old(p) on rows y0-1..y0+8, x0-4..x0+131; H_old(p) on
+// rows y0-1..y0+7, x0-4..x0+127; the material ids of rows y0-1..y0+7,
+// x0-16..x0+127.  Stage t (E(t+1), H(t), ids(t)) completes on its own
+// mbarrier; it is requested two planes ahead, while plane t-2 is computed,
+// into rings of 4 E planes, 3 H planes and 4 id planes.  One CTA per SM
+// (about 132 KB of shared memory).  Fields and H-psi are double-buffered
+// (read E/H/psi_h, write E2/H2/psi_h2), so halo values recomputed here
+// never race with their owners' stores.
+//
+// A cell group takes the fast path when its four cells are all
+// updated; its CPML terms then follow per slab (x: per cell; y: per row;
+// z: per plane; y and z psi as 16-byte accesses).  The E fast path also
+// needs the seven surrounding cells to share one material (ga/gb from a
+// shared-memory copy of the material table).  Every other cell takes the
+// per-cell path with the reference's 4-cell material average.
+//
+// Waits on the mbarriers give up after 2 s of wall time: the CTA then adds
+// to the error counter P.err and returns (the host reports it).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
 
 #include "aem_dev.cuh"
 #include "aem_kernels.h"
 
 namespace aem {
 
-constexpr int Y4_TX = 128, Y4_TY = 8, Y4_ZC = 64;
-constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;  // E tile 136 x 10, x from x0-4
-constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;  // H tile 132 x 9, x from x0-4
-constexpr int Y4_IW = Y4_TX + 16;                    // ids 144 bytes x 9 rows, x from x0-16
-// three rings: E planes k, k+1, k+2; H planes k, k+1; id planes k-1, k, k+1
-constexpr int Y4_ES = 3, Y4_HS = 2, Y4_IS = 3;
-constexpr int Y4_E_B = 3 * Y4_ER * Y4_EW * 4, Y4_H_B = 3 * Y4_HR * Y4_HW * 4, Y4_I_B = Y4_HR * Y4_IW;
+constexpr int Y4_TX = 128, Y4_TY = 8, Y4_ZC = 64, Y4_NT = 32 * (Y4_TY + 1);
+constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;   // E box 136 x 10, x from x0-4, y from y0-1
+constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;   // H box 132 x 9
+constexpr int Y4_IW = Y4_TX + 16, Y4_IR = Y4_TY + 1;  // id box 144 x 9 bytes, x from x0-16
+// every TMA destination starts on a 128-byte boundary
+constexpr int y4_up128(int b) { return (b + 127) / 128 * 128; }
+constexpr int Y4_EC = y4_up128(Y4_ER * Y4_EW * 4) / 4;  // floats from one E component tile to the next
+constexpr int Y4_HC = y4_up128(Y4_HR * Y4_HW * 4) / 4;
+constexpr int Y4_IC = y4_up128(Y4_IR * Y4_IW);          // bytes from one id tile to the next
+// copies run Y4_LA planes ahead: stage t (E(t+1), H(t), ids(t)) is requested
+// at plane t-Y4_LA and consumed at plane t; ring depths in planes follow
+constexpr int Y4_LA = 2;
+constexpr int Y4_ES = Y4_LA + 2, Y4_HS = Y4_LA + 1, Y4_IS = Y4_LA + 2, Y4_NB = Y4_LA + 1;
+constexpr int Y4_OFF_H = Y4_ES * 3 * Y4_EC * 4;
+constexpr int Y4_OFF_I = Y4_OFF_H + Y4_HS * 3 * Y4_HC * 4;
+constexpr int Y4_OFF_HN = Y4_OFF_I + Y4_IS * Y4_IC;
 constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+7
-constexpr int Y4_NMAT = AEM_MAX_MATERIALS;
-constexpr size_t Y4_OFF_H = (size_t)Y4_ES * Y4_E_B, Y4_OFF_I = Y4_OFF_H + (size_t)Y4_HS * Y4_H_B;
-constexpr size_t Y4_OFF_HN = Y4_OFF_I + (size_t)Y4_IS * Y4_I_B;
-constexpr size_t Y4_SMEM = Y4_OFF_HN + (size_t)Y4_HN_F * 4 + (size_t)Y4_NMAT * 6 * 4;
-static_assert(Y4_E_B % 16 == 0 && Y4_H_B % 16 == 0 && Y4_I_B % 16 == 0, "tiles must stay 16-byte aligned");
+constexpr int Y4_OFF_DZ = Y4_OFF_HN + Y4_HN_F * 4;
+constexpr int Y4_OFF_DX = Y4_OFF_DZ + 2 * Y4_ZC * 4;
+constexpr int Y4_OFF_GAB = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
+constexpr int Y4_OFF_BAR = Y4_OFF_GAB + AEM_MAX_MATERIALS * 6 * 4;
+constexpr int Y4_SMEM = Y4_OFF_BAR + Y4_NB * 8;
+constexpr unsigned Y4_TX_E = Y4_ER * Y4_EW * 4, Y4_TX_H = Y4_HR * Y4_HW * 4, Y4_TX_I = Y4_IR * Y4_IW;
+constexpr unsigned Y4_TX_STAGE = 3 * Y4_TX_E + 3 * Y4_TX_H + Y4_TX_I;          // E(t+1), H(t), ids(t)
+constexpr unsigned Y4_TX_FIRST = 9 * Y4_TX_E + 6 * Y4_TX_H + 2 * Y4_TX_I;      // E(z0-1..z0+1), H, ids(z0-1..z0)
+static_assert(Y4_OFF_H % 128 == 0 && Y4_OFF_I % 128 == 0 && Y4_OFF_HN % 128 == 0 && Y4_OFF_BAR % 8 == 0, "layout");
+static_assert(Y4_TX_FIRST < (1u << 20), "mbarrier transaction count");
+static_assert(Y4_SMEM <= 227 * 1024, "shared memory per CTA");
+
+// tensor maps of the current read buffers (3-D: x = pitch PX, y = SY, z = SZ)
+struct Y4Maps {
+    CUtensorMap e[3], h[3], id;
+};
+
+// ---- shared memory, mbarriers and TMA ----
+__device__ __forceinline__ unsigned y4_sa(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void y4_bar_init(uint64_t* b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(y4_sa(b)) : "memory");
+}
+__device__ __forceinline__ void y4_bar_expect(uint64_t* b, unsigned tx) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(y4_sa(b)), "r"(tx) : "memory");
+}
+__device__ __forceinline__ bool y4_bar_try(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(y4_sa(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long y4_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// wait for phase `parity` of barrier b; false after 2 s of wall time
+__device__ __forceinline__ bool y4_bar_wait(uint64_t* b, unsigned parity) {
+    if (y4_bar_try(b, parity)) return true;
+    const unsigned long long t0 = y4_ns();
+    while (!y4_bar_try(b, parity))
+        if (y4_ns() - t0 > 2000000000ull) return false;
+    return true;
+}
+// one box of plane z (z outside 0..SZ-1: zero fill) at (x, y) into dst
+__device__ __forceinline__ void y4_tma(void* dst, const CUtensorMap* m, int x, int y, int z, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(y4_sa(dst)),
+        "l"(m), "r"(x), "r"(y), "r"(z), "r"(y4_sa(b))
+        : "memory");
+}
 
 __device__ inline float ldf4(const void* b, long long i) { return reinterpret_cast<const float*>(b)[i]; }
 __device__ inline void stf4(void* b, long long i, float v) { reinterpret_cast<float*>(b)[i] = v; }
-__device__ inline float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-
-__device__ inline void cp16b(void* smem, const void* gmem, bool valid) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
-}
-__device__ inline void cp_commit4() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ inline void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ inline float psi4(const void* rd, void* wr, bool store, float b, float c, float diff, float dl, long long q) {
-    const float nw = b * ldf4(rd, q) + c * diff / dl;
+    const float nw = b * ldf4(rd, q) + cpml_div(c * diff, dl);
     if (store) stf4(wr, q, nw);
     return nw;
 }
 
-// request the tiles of plane p (wrapped; -1 / SZ = absent): E into `E`,
-// H into `H`, ids into `I` (a null destination skips that tile)
-__device__ inline void y4_issue(const AemParams& P, float* E, float* H, unsigned char* I, int p, int x0, int y0) {
-    const bool pv = p >= 0 && p < P.SZ;
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    const int nE = E ? 3 * Y4_ER * (Y4_EW / 4) : 0, nH = H ? 3 * Y4_HR * (Y4_HW / 4) : 0, nI = I ? Y4_HR * (Y4_IW / 16) : 0;
-    const long long pbase = pv ? (long long)p * P.plane : 0;
-    for (int q = tid; q < nE + nH + nI; q += nt) {
-        if (q < nE) {
-            const int c = q / (Y4_ER * (Y4_EW / 4)), r = (q / (Y4_EW / 4)) % Y4_ER, ch = q % (Y4_EW / 4);
-            const int x = x0 - 4 + 4 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 4 <= P.PX && y >= 0 && y < P.SY;
-            const float* src = reinterpret_cast<const float*>(P.E[c]) + (ok ? pbase + (long long)y * P.PX + x : 0);
-            cp16b(E + (c * Y4_ER + r) * Y4_EW + 4 * ch, src, ok);
-        } else if (q < nE + nH) {
-            const int t = q - nE;
-            const int c = t / (Y4_HR * (Y4_HW / 4)), r = (t / (Y4_HW / 4)) % Y4_HR, ch = t % (Y4_HW / 4);
-            const int x = x0 - 4 + 4 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 4 <= P.PX && y >= 0 && y < P.SY;
-            const float* src = reinterpret_cast<const float*>(P.H[c]) + (ok ? pbase + (long long)y * P.PX + x : 0);
-            cp16b(H + (c * Y4_HR + r) * Y4_HW + 4 * ch, src, ok);
-        } else {
-            const int t = q - nE - nH;
-            const int r = t / (Y4_IW / 16), ch = t % (Y4_IW / 16);
-            const int x = x0 - 16 + 16 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 16 <= P.PX && y >= 0 && y < P.SY;
-            const unsigned char* src = P.cell + (ok ? pbase + (long long)y * P.PX + x : 0);
-            cp16b(I + r * Y4_IW + 16 * ch, src, ok);
-        }
+// one CPML term over four x-contiguous cells (y or z slab: same depth for
+// all four): psi = b psi + c diff / dl (psi from rd; to wr when store, for
+// the cells of mask mk); f += g psi, lane by lane.  The caller passes a
+// non-empty mask only for groups with an updated cell, whose 16 bytes lie
+// inside the psi row (x < pitch).
+__device__ __forceinline__ void y4_psi_row(const void* rd, void* wr, bool store, unsigned mk, float b, float c, float dl,
+                                           long long q, const float d[4], float g, float f[4]) {
+    if (!mk) return;
+    const float4 o = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(rd) + q);
+    const float ov[4] = {o.x, o.y, o.z, o.w};
+    float nw[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        nw[e] = b * ov[e] + cpml_div(c * d[e], dl);
+        f[e] = f[e] + g * nw[e];
+    }
+    if (!store) return;
+    float* w = reinterpret_cast<float*>(wr) + q;
+    if (mk == 0xFu) {
+        *reinterpret_cast<float4*>(w) = make_float4(nw[0], nw[1], nw[2], nw[3]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            if (mk >> e & 1u) w[e] = nw[e];
+    }
+}
+
+// store the cells of mask mk of a 4-cell group (16 bytes when all four)
+__device__ __forceinline__ void y4_store4(void* base, long long c, unsigned mk, const float v[4]) {
+    float* w = reinterpret_cast<float*>(base) + c;
+    if (mk == 0xFu) {
+        *reinterpret_cast<float4*>(w) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            if (mk >> e & 1u) w[e] = v[e];
     }
 }
 
 // H_new of one cell (k_update_h's expressions; psi from psi_h, to psi_h2 when store)
-__device__ __noinline__ float3 y4_h_cell(const AemParams& P, int px, int py, int pz, float ex, float ey, float ez,
+__device__ __forceinline__ float3 y4_h_cell(const AemParams& P, int px, int py, int pz, float ex, float ey, float ez,
                                           float ex_jp, float ez_jp, float ey_ip, float ez_ip, float ex_kp, float ey_kp,
                                           float hx0, float hy0, float hz0, bool store) {
     const int i = px + 1, j = py + 1, k = pz + 1;
@@ -122,47 +200,44 @@ __device__ __noinline__ float3 y4_h_cell(const AemParams& P, int px, int py, int
     return make_float3(hxv, hyv, hzv);
 }
 
-// Ga/Gb of an E edge from its four cell ids (reference order, ref :2516-2527)
-// CPML terms of one H cell added to bulk values (the k_update_h order:
-// Hx y then z, Hy x then z, Hz x then y)
-__device__ __noinline__ float3 y4_h_pml(const AemParams& P, int px, int py, int pz, float dzy, float dyz, float dzx,
-                                        float dxz, float dyx, float dxy, bool store, float hxv, float hyv, float hzv) {
-    // dzy = ez - ez_jp, dyz = ey_kp - ey, dzx = ez_ip - ez, dxz = ex - ex_kp, dyx = ey - ey_ip, dxy = ex_jp - ex
-    const int i = px + 1, j = py + 1, k = pz + 1;
+// x-slab CPML terms of one H cell (Hy, Hz), added before the y and z terms
+__device__ __forceinline__ float2 y4_h_xpml(const AemParams& P, int px, int py, int pz, float dzx, float dyx, bool store,
+                                         float hyv, float hzv) {
+    // dzx = ez_ip - ez, dyx = ey - ey_ip
+    const int i = px + 1;
     const float DB = P.DB;
     const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
-    const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
-    const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-    if (qy_lo) hxv = hxv + DB * psi4(P.psi_h[0][1][0], P.psi_h2[0][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], dzy, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-    if (qy_hi) hxv = hxv + DB * psi4(P.psi_h[0][1][1], P.psi_h2[0][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], dzy, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-    if (qz_lo) hxv = hxv + DB * psi4(P.psi_h[0][2][0], P.psi_h2[0][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], dyz, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-    if (qz_hi) hxv = hxv + DB * psi4(P.psi_h[0][2][1], P.psi_h2[0][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], dyz, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-    if (qx_lo) hyv = hyv + DB * psi4(P.psi_h[1][0][0], P.psi_h2[1][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dzx, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-    if (qx_hi) hyv = hyv + DB * psi4(P.psi_h[1][0][1], P.psi_h2[1][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dzx, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-    if (qz_lo) hyv = hyv + DB * psi4(P.psi_h[1][2][0], P.psi_h2[1][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], dxz, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-    if (qz_hi) hyv = hyv + DB * psi4(P.psi_h[1][2][1], P.psi_h2[1][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], dxz, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-    if (qx_lo) hzv = hzv + DB * psi4(P.psi_h[2][0][0], P.psi_h2[2][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dyx, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-    if (qx_hi) hzv = hzv + DB * psi4(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dyx, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-    if (qy_lo) hzv = hzv + DB * psi4(P.psi_h[2][1][0], P.psi_h2[2][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], dxy, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-    if (qy_hi) hzv = hzv + DB * psi4(P.psi_h[2][1][1], P.psi_h2[2][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], dxy, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-    return make_float3(hxv, hyv, hzv);
+    if (qx_lo) {
+        const long long q = psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]);
+        hyv = hyv + DB * psi4(P.psi_h[1][0][0], P.psi_h2[1][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dzx, P.del[0], q);
+        hzv = hzv + DB * psi4(P.psi_h[2][0][0], P.psi_h2[2][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dyx, P.del[0], q);
+    }
+    if (qx_hi) {
+        const long long q = psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]);
+        hyv = hyv + DB * psi4(P.psi_h[1][0][1], P.psi_h2[1][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dzx, P.del[0], q);
+        hzv = hzv + DB * psi4(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dyx, P.del[0], q);
+    }
+    return make_float2(hyv, hzv);
 }
 
-// CPML terms of one E cell and component added to its bulk value
-__device__ __noinline__ float y4_e_pml(const AemParams& P, int comp, int px, int py, int pz, float e, float gb, float d1,
-                                       float d2) {
-    const int i = px + 1, j = py + 1, k = pz + 1;
+// x-slab CPML terms of one E cell (Ey, Ez), added before the y and z terms;
+// psi of a component that is not updated (uy / uz false) is left alone
+__device__ __forceinline__ float2 y4_e_xpml(const AemParams& P, int px, int py, int pz, float dzx, float dyx, float gby,
+                                            float gbz, bool uy, bool uz, float eyv, float ezv) {
+    // dzx = hz(i-1) - hz (Ey), dyx = hy - hy(i-1) (Ez)
+    const int i = px + 1;
     const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
-    const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
-    const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
-    const int a1 = comp == 0 ? 1 : 0, a2 = comp == 2 ? 1 : 2;
-    const int q1l = a1 == 0 ? qxl : qyl, q1h = a1 == 0 ? qxh : qyh;
-    const int q2l = a2 == 1 ? qyl : qzl, q2h = a2 == 1 ? qyh : qzh;
-    if (q1l) e = e + gb * psi4(P.psi_e[comp][a1][0], P.psi_e[comp][a1][0], true, P.be[a1][0][q1l - 1], P.ce[a1][0][q1l - 1], d1, P.del[a1], psi_idx(P, a1, q1l, px, py, pz, P.npml[a1][0]));
-    if (q1h) e = e + gb * psi4(P.psi_e[comp][a1][1], P.psi_e[comp][a1][1], true, P.be[a1][1][q1h - 1], P.ce[a1][1][q1h - 1], d1, P.del[a1], psi_idx(P, a1, q1h, px, py, pz, P.npml[a1][1]));
-    if (q2l) e = e + gb * psi4(P.psi_e[comp][a2][0], P.psi_e[comp][a2][0], true, P.be[a2][0][q2l - 1], P.ce[a2][0][q2l - 1], d2, P.del[a2], psi_idx(P, a2, q2l, px, py, pz, P.npml[a2][0]));
-    if (q2h) e = e + gb * psi4(P.psi_e[comp][a2][1], P.psi_e[comp][a2][1], true, P.be[a2][1][q2h - 1], P.ce[a2][1][q2h - 1], d2, P.del[a2], psi_idx(P, a2, q2h, px, py, pz, P.npml[a2][1]));
-    return e;
+    if (qxl) {
+        const long long q = psi_idx(P, 0, qxl, px, py, pz, P.npml[0][0]);
+        if (uy) eyv = eyv + gby * psi4(P.psi_e[1][0][0], P.psi_e[1][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], dzx, P.del[0], q);
+        if (uz) ezv = ezv + gbz * psi4(P.psi_e[2][0][0], P.psi_e[2][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], dyx, P.del[0], q);
+    }
+    if (qxh) {
+        const long long q = psi_idx(P, 0, qxh, px, py, pz, P.npml[0][1]);
+        if (uy) eyv = eyv + gby * psi4(P.psi_e[1][0][1], P.psi_e[1][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], dzx, P.del[0], q);
+        if (uz) ezv = ezv + gbz * psi4(P.psi_e[2][0][1], P.psi_e[2][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], dyx, P.del[0], q);
+    }
+    return make_float2(eyv, ezv);
 }
 
 __device__ inline void y4_gagb(const AemParams& P, const float* gab, int c, int i0, int i1, int i2, int i3, float& ga,
@@ -180,95 +255,9 @@ __device__ inline void y4_gagb(const AemParams& P, const float* gab, int c, int 
     gb = d_gb(s + tp, e, P.dt);
 }
 
-// H_new of the thread's four cells (row r of the tile, x = xb..xb+3) from
-// plane slots E0 (k), E1 (k+1), Ho (H_old k); non-updated cells keep H_old.
-// Owned cells (store) also go to H2 / psi_h2.
-__device__ inline void y4_h_group(const AemParams& P, const float* E0, const float* E1, const float* Ho, int r, int xi,
-                                  int xb, int py, int pz, int hxm, int hym, int hzm, bool store, float hx[4], float hy[4],
-                                  float hz[4]) {
-    const float* Ex = E0 + (0 * Y4_ER + r) * Y4_EW;
-    const float* Ey = E0 + (1 * Y4_ER + r) * Y4_EW;
-    const float* Ez = E0 + (2 * Y4_ER + r) * Y4_EW;
-    const float4 ex = lds4(Ex + xi), ey = lds4(Ey + xi), ez = lds4(Ez + xi);
-    const float4 exj = lds4(Ex + Y4_EW + xi), ezj = lds4(Ez + Y4_EW + xi);
-    const float ey4 = Ey[xi + 4], ez4 = Ez[xi + 4];
-    const float4 exk = lds4(E1 + (0 * Y4_ER + r) * Y4_EW + xi), eyk = lds4(E1 + (1 * Y4_ER + r) * Y4_EW + xi);
-    const float4 h0x = lds4(Ho + (0 * Y4_HR + r) * Y4_HW + xi), h0y = lds4(Ho + (1 * Y4_HR + r) * Y4_HW + xi),
-                 h0z = lds4(Ho + (2 * Y4_HR + r) * Y4_HW + xi);
-    const float vex[4] = {ex.x, ex.y, ex.z, ex.w}, vey[4] = {ey.x, ey.y, ey.z, ey.w}, vez[4] = {ez.x, ez.y, ez.z, ez.w};
-    const float vexj[4] = {exj.x, exj.y, exj.z, exj.w}, vezj[4] = {ezj.x, ezj.y, ezj.z, ezj.w};
-    const float veyi[4] = {ey.y, ey.z, ey.w, ey4}, vezi[4] = {ez.y, ez.z, ez.w, ez4};
-    const float vexk[4] = {exk.x, exk.y, exk.z, exk.w}, veyk[4] = {eyk.x, eyk.y, eyk.z, eyk.w};
-    const float vhx[4] = {h0x.x, h0x.y, h0x.z, h0x.w}, vhy[4] = {h0y.x, h0y.y, h0y.z, h0y.w},
-                vhz[4] = {h0z.x, h0z.y, h0z.z, h0z.w};
-    const int i0 = xb + 1, j = py + 1, k = pz + 1;
-    const bool upd_all = xb + 3 <= hxm && py >= 0 && py <= hym && pz <= hzm;
-    const bool no_pml = i0 >= P.npml[0][0] && xb + 4 <= P.X - P.npml[0][1] && j >= P.npml[1][0] &&
-                        j <= P.Y - P.npml[1][1] && k >= P.npml[2][0] && k <= P.Z - P.npml[2][1];
-    if (upd_all) {
-        const float DB = P.DB, dhy = P.den_h[1][j - 1], dhz = P.den_h[2][k - 1];
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const float dhx = P.den_h[0][i0 + e - 1];
-            hx[e] = vhx[e] + DB * ((vez[e] - vezj[e]) * dhy + (veyk[e] - vey[e]) * dhz);
-            hy[e] = vhy[e] + DB * ((vezi[e] - vez[e]) * dhx + (vex[e] - vexk[e]) * dhz);
-            hz[e] = vhz[e] + DB * ((vey[e] - veyi[e]) * dhx + (vexj[e] - vex[e]) * dhy);
-        }
-        if (!no_pml) {
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-            {
-                const float3 h = y4_h_pml(P, xb + e, py, pz, vez[e] - vezj[e], veyk[e] - vey[e], vezi[e] - vez[e],
-                                          vex[e] - vexk[e], vey[e] - veyi[e], vexj[e] - vex[e], store, hx[e], hy[e], hz[e]);
-                hx[e] = h.x; hy[e] = h.y; hz[e] = h.z;
-            }
-        }
-        if (store) {
-            const long long c = lin(P, xb, py, pz);
-            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[0]) + c) = make_float4(hx[0], hx[1], hx[2], hx[3]);
-            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[1]) + c) = make_float4(hy[0], hy[1], hy[2], hy[3]);
-            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[2]) + c) = make_float4(hz[0], hz[1], hz[2], hz[3]);
-        }
-        return;
-    }
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        const int px = xb + e;
-        hx[e] = vhx[e]; hy[e] = vhy[e]; hz[e] = vhz[e];
-        if (px <= hxm && py >= 0 && py <= hym && pz <= hzm) {
-            const float3 h = y4_h_cell(P, px, py, pz, vex[e], vey[e], vez[e], vexj[e], vezj[e], veyi[e], vezi[e], vexk[e],
-                                       veyk[e], vhx[e], vhy[e], vhz[e], store);
-            hx[e] = h.x; hy[e] = h.y; hz[e] = h.z;
-            if (store) {
-                const long long c = lin(P, px, py, pz);
-                stf4(P.H2[0], c, hx[e]);
-                stf4(P.H2[1], c, hy[e]);
-                stf4(P.H2[2], c, hz[e]);
-            }
-        }
-    }
-}
-
-// the -x halo cell (x0-1, py) of a row: Hy, Hz (never stored)
-__device__ __noinline__ float2 y4_h_xhalo(const AemParams& P, const float* E0, const float* E1, const float* Ho, int r,
-                                           int x0, int py, int pz, int hxm, int hym, int hzm) {
-    const int c3 = 3;  // tile column of x0-1
-    const float hyv = Ho[(1 * Y4_HR + r) * Y4_HW + c3];
-    const float hzv = Ho[(2 * Y4_HR + r) * Y4_HW + c3];
-    const int px = x0 - 1;
-    if (px < 0 || px > hxm || py < 0 || py > hym || pz > hzm) return make_float2(hyv, hzv);
-    const float* Ex = E0 + (0 * Y4_ER + r) * Y4_EW;
-    const float* Ey = E0 + (1 * Y4_ER + r) * Y4_EW;
-    const float* Ez = E0 + (2 * Y4_ER + r) * Y4_EW;
-    const float3 h = y4_h_cell(P, px, py, pz, Ex[c3], Ey[c3], Ez[c3], Ex[Y4_EW + c3], Ez[Y4_EW + c3], Ey[c3 + 1],
-                               Ez[c3 + 1], E1[(0 * Y4_ER + r) * Y4_EW + c3], E1[(1 * Y4_ER + r) * Y4_EW + c3],
-                               Ho[(0 * Y4_HR + r) * Y4_HW + c3], hyv, hzv, false);
-    return make_float2(h.y, h.z);
-}
-
 // E_new of one cell and one component (k_update_e's expressions)
 __device__ __noinline__ float y4_e_comp(const AemParams& P, const float* gab, int comp, int px, int py, int pz, float eold,
-                                  float d1, float d2, float den1, float den2, int i0, int i1, int i2, int i3) {
+                                        float d1, float d2, float den1, float den2, int i0, int i1, int i2, int i3) {
     const float curl = d1 * den1 + d2 * den2;
     float ga, gb;
     y4_gagb(P, gab, comp, i0, i1, i2, i3, ga, gb);
@@ -288,137 +277,375 @@ __device__ __noinline__ float y4_e_comp(const AemParams& P, const float* gab, in
     return e;
 }
 
-__global__ void __maxnreg__(112) k_yee4(const __grid_constant__ AemParams P) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);  // [2][9][128]: hx, hz of H_new(k)
-    float* gab = Hn + Y4_HN_F;                              // [mat][6]: ga xyz, gb xyz
+// the -x halo cell (x0-1, py) of a row: Hy, Hz (never stored); dhx is
+// den_h x of x0-1.  A bulk cell is computed here from the tiles; a CPML cell
+// takes the per-cell path.
+__device__ __forceinline__ float2 y4_h_xhalo(const AemParams& P, const float* E0, const float* E1, const float* Ho, int r,
+                                             int x0, int py, int pz, int hzm, bool cpml_yz, float dhx, float dhy,
+                                             float dhz) {
+    const int c3 = 3;  // tile column of x0-1
+    const float hyv = Ho[1 * Y4_HC + r * Y4_HW + c3];
+    const float hzv = Ho[2 * Y4_HC + r * Y4_HW + c3];
+    const int px = x0 - 1, i = x0;
+    if (px < 0 || px > P.SX - 2 || py < 0 || py > P.SY - 2 || pz > hzm) return make_float2(hyv, hzv);
+    const float* Ex = E0 + 0 * Y4_EC + r * Y4_EW;
+    const float* Ey = E0 + 1 * Y4_EC + r * Y4_EW;
+    const float* Ez = E0 + 2 * Y4_EC + r * Y4_EW;
+    const float ex = Ex[c3], ey = Ey[c3], ez = Ez[c3];
+    const float ex_jp = Ex[Y4_EW + c3], ey_ip = Ey[c3 + 1], ez_ip = Ez[c3 + 1];
+    const float ex_kp = E1[0 * Y4_EC + r * Y4_EW + c3];
+    if (!cpml_yz && i > P.npml[0][0] - 1 && i < P.X + 1 - P.npml[0][1]) {
+        const float DB = P.DB;
+        return make_float2(hyv + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz),
+                           hzv + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy));
+    }
+    const float3 h = y4_h_cell(P, px, py, pz, ex, ey, ez, ex_jp, Ez[Y4_EW + c3], ey_ip, ez_ip, ex_kp,
+                               E1[1 * Y4_EC + r * Y4_EW + c3], Ho[0 * Y4_HC + r * Y4_HW + c3], hyv, hzv, false);
+    return make_float2(h.y, h.z);
+}
+
+// per-thread constants of the z march
+struct Y4Row {
+    int r, py, xb, xi, xbi;
+    bool own;        // warps 0..7 on a stored row
+    bool hrow;       // the row computes H (own rows and the -y halo row)
+    unsigned hmask;  // cells of the group inside the H update range in x and y (bit e: cell xb+e)
+    bool h_xpml;     // a cell of the group lies in an x CPML slab (H)
+    int qyh_lo, qyh_hi;  // y CPML depth of the row (H), 0 outside
+    unsigned emx, emy, emz;  // cells whose Ex / Ey / Ez is updated, as far as x and y decide
+    bool unavg_xy;   // a cell of the group has i == 1 or j == 1 (no material averaging)
+    bool e_xpml;     // a cell of the group lies in an x CPML slab (E)
+    int qye_lo, qye_hi;  // y CPML depth of the row (E)
+    long long rowoff;    // py * PX + xb
+};
+
+// H_new of the thread's four cells (row r of the tile) from E0 (plane k),
+// E1 (k+1), Ho (H_old k); non-updated cells keep H_old.  `store`: write to
+// H2 / psi_h2 (owned cells).
+__device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, const float* E0, const float* E1,
+                                           const float* Ho, int pz, int hzm, float dhz, const float* dxs, float dhy,
+                                           bool store, float hx[4], float hy[4], float hz[4]) {
+    const float* Ex = E0 + 0 * Y4_EC + T.r * Y4_EW;
+    const float* Ey = E0 + 1 * Y4_EC + T.r * Y4_EW;
+    const float* Ez = E0 + 2 * Y4_EC + T.r * Y4_EW;
+    const float4 ex = lds4(Ex + T.xi), ey = lds4(Ey + T.xi), ez = lds4(Ez + T.xi);
+    const float4 exj = lds4(Ex + Y4_EW + T.xi), ezj = lds4(Ez + Y4_EW + T.xi);
+    const float ey4 = Ey[T.xi + 4], ez4 = Ez[T.xi + 4];
+    const float4 exk = lds4(E1 + 0 * Y4_EC + T.r * Y4_EW + T.xi), eyk = lds4(E1 + 1 * Y4_EC + T.r * Y4_EW + T.xi);
+    const float4 h0x = lds4(Ho + 0 * Y4_HC + T.r * Y4_HW + T.xi), h0y = lds4(Ho + 1 * Y4_HC + T.r * Y4_HW + T.xi),
+                 h0z = lds4(Ho + 2 * Y4_HC + T.r * Y4_HW + T.xi);
+    const float vex[4] = {ex.x, ex.y, ex.z, ex.w}, vey[4] = {ey.x, ey.y, ey.z, ey.w}, vez[4] = {ez.x, ez.y, ez.z, ez.w};
+    const float vexj[4] = {exj.x, exj.y, exj.z, exj.w}, vezj[4] = {ezj.x, ezj.y, ezj.z, ezj.w};
+    const float veyi[4] = {ey.y, ey.z, ey.w, ey4}, vezi[4] = {ez.y, ez.z, ez.w, ez4};
+    const float vexk[4] = {exk.x, exk.y, exk.z, exk.w}, veyk[4] = {eyk.x, eyk.y, eyk.z, eyk.w};
+    const float vhx[4] = {h0x.x, h0x.y, h0x.z, h0x.w}, vhy[4] = {h0y.x, h0y.y, h0y.z, h0y.w},
+                vhz[4] = {h0z.x, h0z.y, h0z.z, h0z.w};
+    // cells of the group inside the H update range (all four in the bulk)
+    const unsigned mk = pz <= hzm ? T.hmask : 0u;
+    if (!mk) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) { hx[e] = vhx[e]; hy[e] = vhy[e]; hz[e] = vhz[e]; }
+        return;
+    }
+    const float DB = P.DB;
+    const float4 dx4 = lds4(dxs + 4 * (T.xi / 4 - 1));
+    const float dhx[4] = {dx4.x, dx4.y, dx4.z, dx4.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        hx[e] = vhx[e] + DB * ((vez[e] - vezj[e]) * dhy + (veyk[e] - vey[e]) * dhz);
+        hy[e] = vhy[e] + DB * ((vezi[e] - vez[e]) * dhx[e] + (vex[e] - vexk[e]) * dhz);
+        hz[e] = vhz[e] + DB * ((vey[e] - veyi[e]) * dhx[e] + (vexj[e] - vex[e]) * dhy);
+    }
+    // CPML terms in the reference's order: Hx (y, z), Hy (x, z), Hz (x, y)
+    if (T.h_xpml) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if (!(mk >> e & 1u)) continue;
+            const float2 t = y4_h_xpml(P, T.xb + e, T.py, pz, vezi[e] - vez[e], vey[e] - veyi[e], store, hy[e], hz[e]);
+            hy[e] = t.x; hz[e] = t.y;
+        }
+    }
+    if (T.qyh_lo | T.qyh_hi) {
+        float dzy[4], dxy[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) { dzy[e] = vez[e] - vezj[e]; dxy[e] = vexj[e] - vex[e]; }
+        for (int s = 0; s < 2; s++) {
+            const int q = s ? T.qyh_hi : T.qyh_lo;
+            if (!q) continue;
+            const int n = P.npml[1][s];
+            const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
+            y4_psi_row(P.psi_h[0][1][s], P.psi_h2[0][1][s], store, mk, P.bh[1][s][q - 1], P.ch[1][s][q - 1], P.del[1], o, dzy, DB, hx);
+            y4_psi_row(P.psi_h[2][1][s], P.psi_h2[2][1][s], store, mk, P.bh[1][s][q - 1], P.ch[1][s][q - 1], P.del[1], o, dxy, DB, hz);
+        }
+    }
+    const int k = pz + 1;
+    const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
+    if (qz_lo | qz_hi) {
+        float dyz[4], dxz[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) { dyz[e] = veyk[e] - vey[e]; dxz[e] = vex[e] - vexk[e]; }
+        for (int s = 0; s < 2; s++) {
+            const int q = s ? qz_hi : qz_lo;
+            if (!q) continue;
+            const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
+            y4_psi_row(P.psi_h[0][2][s], P.psi_h2[0][2][s], store, mk, P.bh[2][s][q - 1], P.ch[2][s][q - 1], P.del[2], o, dyz, DB, hx);
+            y4_psi_row(P.psi_h[1][2][s], P.psi_h2[1][2][s], store, mk, P.bh[2][s][q - 1], P.ch[2][s][q - 1], P.del[2], o, dxz, DB, hy);
+        }
+    }
+    if (mk != 0xFu) {
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            if (!(mk >> e & 1u)) { hx[e] = vhx[e]; hy[e] = vhy[e]; hz[e] = vhz[e]; }
+    }
+    if (store) {
+        const long long c = (long long)pz * P.plane + T.rowoff;
+        y4_store4(P.H2[0], c, mk, hx);
+        y4_store4(P.H2[1], c, mk, hy);
+        y4_store4(P.H2[2], c, mk, hz);
+    }
+}
+
+__global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemParams P, const __grid_constant__ Y4Maps M) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);    // [2][9][128]: hx, hz of H_new(k)
+    float* dzs = reinterpret_cast<float*>(smem + Y4_OFF_DZ);   // den_h z, den_e z of the chunk's planes
+    float* dxs = reinterpret_cast<float*>(smem + Y4_OFF_DX);   // den_h x, den_e x of the tile's columns
+    float* gab = reinterpret_cast<float*>(smem + Y4_OFF_GAB);  // [mat][6]: ga xyz, gb xyz
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Y4_OFF_BAR);
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int tid = lane + 32 * w, nthr = 32 * (Y4_TY + 1);
+    const int tid = lane + 32 * w;
     const int x0 = blockIdx.x * Y4_TX, y0 = blockIdx.y * Y4_TY;
     const int z0 = blockIdx.z * Y4_ZC, z1 = min(P.SZ, z0 + Y4_ZC);
-    const int hxm = P.SX - 2, hym = P.SY - 2, hzm = P.per[2] ? P.SZ - 1 : P.SZ - 2;
+    const int hzm = P.per[2] ? P.SZ - 1 : P.SZ - 2;
     const unsigned FULL = 0xffffffffu;
-    for (int q = tid; q < P.nmat * 6; q += nthr) {
-        const int m = q / 6, c = q % 6;
-        gab[q] = c < 3 ? P.ucoef[m].ga[c] : P.ucoef[m].gb[c - 3];
+    if (y4_sa(smem) & 127) {  // the TMA boxes need 128-byte aligned destinations
+        if (tid == 0) atomicAdd(P.err, 1);
+        return;
     }
     auto zw = [&](int p) { return P.per[2] ? (p % P.SZ + P.SZ) % P.SZ : p; };
     auto md = [](int p, int m) { return ((p % m) + m) % m; };
-    auto Ew = [&](int p) { return reinterpret_cast<float*>(smem + (size_t)md(p, Y4_ES) * Y4_E_B); };
-    auto Hw = [&](int p) { return reinterpret_cast<float*>(smem + Y4_OFF_H + (size_t)md(p, Y4_HS) * Y4_H_B); };
-    auto Iw = [&](int p) { return smem + Y4_OFF_I + (size_t)md(p, Y4_IS) * Y4_I_B; };
-    auto Es = [&](int p) { return (const float*)Ew(p); };
-    auto Hs = [&](int p) { return (const float*)Hw(p); };
-    auto Is = [&](int p) { return (const unsigned char*)Iw(p); };
-
-    // this thread's cells: tile row r (0 = the -y halo row), x = xb..xb+3
-    const int r = w == Y4_TY ? 0 : w + 1;
-    const int py = y0 - 1 + r;
-    const int xb = x0 + 4 * lane, xi = 4 * lane + 4, xbi = 4 * lane + 16;
-    const bool own = w < Y4_TY && py < P.SY;
-
+    auto Ew = [&](int p) { return reinterpret_cast<float*>(smem + md(p, Y4_ES) * 3 * Y4_EC * 4); };
+    auto Hw = [&](int p) { return reinterpret_cast<float*>(smem + Y4_OFF_H + md(p, Y4_HS) * 3 * Y4_HC * 4); };
+    auto Iw = [&](int p) { return smem + Y4_OFF_I + md(p, Y4_IS) * Y4_IC; };
+    // E (3 boxes), H (3) and ids (1) of plane p into the given slots (null: skipped)
+    auto issue = [&](float* E, float* H, unsigned char* I, int p, uint64_t* b) {
+        for (int c = 0; c < 3; c++)
+            if (E) y4_tma(E + c * Y4_EC, &M.e[c], x0 - 4, y0 - 1, p, b);
+        for (int c = 0; c < 3; c++)
+            if (H) y4_tma(H + c * Y4_HC, &M.h[c], x0 - 4, y0 - 1, p, b);
+        if (I) y4_tma(I, &M.id, x0 - 16, y0 - 1, p, b);
+    };
     const bool below = P.per[2] || z0 > 0;
-    // prologue: E of planes z0-1..z0+1, H and ids of z0-1 and z0
-    y4_issue(P, Ew(z0 - 1), Hw(z0 - 1), Iw(z0 - 1), below ? zw(z0 - 1) : -1, x0, y0);
-    y4_issue(P, Ew(z0), Hw(z0), Iw(z0), zw(z0), x0, y0);
-    y4_issue(P, Ew(z0 + 1), nullptr, nullptr, zw(z0 + 1), x0, y0);
-    cp_commit4();
-    cp_wait0();
+    auto pz_of = [&](int p) { return (p < 0 || p >= P.SZ) && !P.per[2] ? -1 : zw(p); };  // -1: zero fill
+
+    if (tid == 0) {
+        for (int b = 0; b < Y4_NB; b++) y4_bar_init(&bar[b]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int q = tid; q < P.nmat * 6; q += Y4_NT) {
+        const int m = q / 6, c = q % 6;
+        gab[q] = c < 3 ? P.ucoef[m].ga[c] : P.ucoef[m].gb[c - 3];
+    }
+    for (int q = tid; q < z1 - z0; q += Y4_NT) {
+        dzs[q] = P.den_h[2][zw(z0 + q)];
+        dzs[Y4_ZC + q] = P.den_e[2][zw(z0 + q)];
+    }
+    for (int q = tid; q < Y4_TX; q += Y4_NT) {
+        const bool in = x0 + q < P.SX;
+        dxs[q] = in ? P.den_h[0][x0 + q] : 0.0f;
+        dxs[Y4_TX + q] = in ? P.den_e[0][x0 + q] : 0.0f;
+    }
+    if (tid == 0) dxs[2 * Y4_TX] = x0 >= 1 ? P.den_h[0][x0 - 1] : 0.0f;
     __syncthreads();
+    if (tid == 0) {
+        y4_bar_expect(&bar[0], Y4_TX_FIRST);
+        issue(Ew(z0 - 1), Hw(z0 - 1), Iw(z0 - 1), below ? zw(z0 - 1) : -1, &bar[0]);
+        issue(Ew(z0), Hw(z0), Iw(z0), zw(z0), &bar[0]);
+        issue(Ew(z0 + 1), nullptr, nullptr, pz_of(z0 + 1), &bar[0]);
+        for (int t = z0 + 1; t < z0 + Y4_LA && t < z1; t++) {
+            y4_bar_expect(&bar[t - z0], Y4_TX_STAGE);
+            issue(Ew(t + 1), nullptr, nullptr, pz_of(t + 1), &bar[t - z0]);
+            issue(nullptr, Hw(t), Iw(t), zw(t), &bar[t - z0]);
+        }
+    }
+
+    // per-thread constants
+    Y4Row T;
+    T.r = w == Y4_TY ? 0 : w + 1;
+    T.py = y0 - 1 + T.r;
+    T.xb = x0 + 4 * lane;
+    T.xi = 4 * lane + 4;
+    T.xbi = 4 * lane + 16;
+    T.own = w < Y4_TY && T.py < P.SY;
+    T.hrow = T.own || (w == Y4_TY && T.py >= 0);
+    T.rowoff = (long long)T.py * P.PX + T.xb;
+    const int j = T.py + 1, i0 = T.xb + 1;
+    {
+        unsigned hx = 0, ex = 0, eyz = 0;
+        for (int e = 0; e < 4; e++) {
+            const int px = T.xb + e;
+            if (px <= P.SX - 2) { hx |= 1u << e; ex |= 1u << e; }
+            if (px >= 1 && px <= P.SX - 2) eyz |= 1u << e;
+        }
+        const bool rx = T.py >= 1 && T.py <= P.SY - 2, ry = T.py >= 0 && T.py <= P.SY - 2;
+        T.hmask = ry ? hx : 0u;
+        T.emx = rx ? ex : 0u;
+        T.emy = ry ? eyz : 0u;
+        T.emz = rx ? eyz : 0u;
+        T.unavg_xy = T.xb == 0 || T.py == 0;
+    }
+    T.h_xpml = i0 <= P.npml[0][0] - 1 || i0 + 3 >= P.X + 1 - P.npml[0][1];
+    T.qyh_lo = (j <= P.npml[1][0] - 1) ? j : 0;
+    T.qyh_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+    T.e_xpml = i0 <= P.npml[0][0] || i0 + 3 >= P.X + 1 - P.npml[0][1];
+    T.qye_lo = (j >= 2 && j <= P.npml[1][0]) ? j : 0;
+    T.qye_hi = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
+    const bool yin = T.py >= 0 && T.py < P.SY;
+    const float dhy = yin ? P.den_h[1][T.py] : 0.0f, dey = yin ? P.den_e[1][T.py] : 0.0f;
+
+    bool ok = y4_bar_wait(&bar[0], 0);
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicAdd(P.err, 1);
+        return;
+    }
     // H_new(z0-1) of the own cells (the plane below belongs to the chunk underneath)
     float hxp[4] = {0, 0, 0, 0}, hyp[4] = {0, 0, 0, 0};
-    if (below && own) {
+    if (below && T.own) {
         float hz_unused[4];
-        y4_h_group(P, Es(z0 - 1), Es(z0), Hs(z0 - 1), r, xi, xb, py, zw(z0 - 1), hxm, hym, hzm, false, hxp, hyp, hz_unused);
+        const int pzb = zw(z0 - 1);
+        y4_h_group(P, T, Ew(z0 - 1), Ew(z0), Hw(z0 - 1), pzb, hzm, P.den_h[2][pzb], dxs, dhy, false, hxp, hyp, hz_unused);
     }
-    const int j = py + 1;
-    const float dey = own ? P.den_e[1][j - 1] : 0.0f;
 
     for (int k = z0; k < z1; k++) {
         const int pz = zw(k);
-        // E(k+1), H(k), ids(k) have landed and every thread is done with
-        // plane k-1: E(k+2), H(k+1), ids(k+1) reuse the slots of E(k-1),
-        // H(k-1), ids(k-2)
-        cp_wait0();
-        __syncthreads();
-        y4_issue(P, Ew(k + 2), nullptr, nullptr, k + 2 <= z1 ? zw(k + 2) : -1, x0, y0);
-        y4_issue(P, nullptr, Hw(k + 1), Iw(k + 1), k + 1 < z1 ? zw(k + 1) : -1, x0, y0);
-        cp_commit4();
+        // stage k (E(k+1), H(k), ids(k)) has landed, and every thread is done
+        // with plane k-1: stage k+Y4_LA reuses the slots of E(k-1), H(k-1),
+        // ids(k-2) and the barrier of stage k-1
+        if (k > z0) ok = y4_bar_wait(&bar[(k - z0) % Y4_NB], ((k - z0) / Y4_NB) & 1);
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) atomicAdd(P.err, 1);
+            return;
+        }
+        if (tid == 0 && k + Y4_LA < z1) {
+            const int t = k + Y4_LA;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            uint64_t* b = &bar[(t - z0) % Y4_NB];
+            y4_bar_expect(b, Y4_TX_STAGE);
+            issue(Ew(t + 1), nullptr, nullptr, pz_of(t + 1), b);
+            issue(nullptr, Hw(t), Iw(t), zw(t), b);
+        }
 
         // ---- H_new(k): own rows, the -y halo row (warp 8), the -x halo cell (lane 0)
-        const float* E0 = Es(k);
+        const float* E0 = Ew(k);
+        const float dhz = dzs[k - z0], dez = dzs[Y4_ZC + k - z0];
         float hx[4], hy[4], hz[4];
-        if (own || (w == Y4_TY && py >= 0))
-            y4_h_group(P, E0, Es(k + 1), Hs(k), r, xi, xb, py, pz, hxm, hym, hzm, own, hx, hy, hz);
+        if (T.hrow)
+            y4_h_group(P, T, E0, Ew(k + 1), Hw(k), pz, hzm, dhz, dxs, dhy, T.own, hx, hy, hz);
         else
             for (int e = 0; e < 4; e++) hx[e] = hy[e] = hz[e] = 0.0f;
         float hy_xh = 0.0f, hz_xh = 0.0f;
-        if (lane == 0 && own) {
-            const float2 hh = y4_h_xhalo(P, E0, Es(k + 1), Hs(k), r, x0, py, pz, hxm, hym, hzm);
+        if (lane == 0 && T.own) {
+            const int kz = pz + 1;
+            const bool cpml_yz = (T.qyh_lo | T.qyh_hi) || kz <= P.npml[2][0] - 1 || kz >= P.Z + 1 - P.npml[2][1];
+            const float2 hh = y4_h_xhalo(P, E0, Ew(k + 1), Hw(k), T.r, x0, T.py, pz, hzm, cpml_yz, dxs[2 * Y4_TX], dhy, dhz);
             hy_xh = hh.x; hz_xh = hh.y;
         }
-        *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
-        *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+        *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+        *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
         __syncthreads();
 
         // ---- E_new(k) of the own rows
         if (w < Y4_TY) {
             float hz_im0 = __shfl_up_sync(FULL, hz[3], 1), hy_im0 = __shfl_up_sync(FULL, hy[3], 1);
             if (lane == 0) { hz_im0 = hz_xh; hy_im0 = hy_xh; }
-            if (own) {
+            if (T.own) {
+                const int r = T.r;
                 const float4 hxj4 = lds4(Hn + (0 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
                 const float4 hzj4 = lds4(Hn + (1 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
                 const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
                 const float him_z[4] = {hz_im0, hz[0], hz[1], hz[2]}, him_y[4] = {hy_im0, hy[0], hy[1], hy[2]};
-                const float4 ex4 = lds4(E0 + (0 * Y4_ER + r) * Y4_EW + xi), ey4 = lds4(E0 + (1 * Y4_ER + r) * Y4_EW + xi),
-                             ez4 = lds4(E0 + (2 * Y4_ER + r) * Y4_EW + xi);
+                const float4 ex4 = lds4(E0 + 0 * Y4_EC + r * Y4_EW + T.xi), ey4 = lds4(E0 + 1 * Y4_EC + r * Y4_EW + T.xi),
+                             ez4 = lds4(E0 + 2 * Y4_EC + r * Y4_EW + T.xi);
                 const float vex[4] = {ex4.x, ex4.y, ex4.z, ex4.w}, vey[4] = {ey4.x, ey4.y, ey4.z, ey4.w},
                             vez[4] = {ez4.x, ez4.y, ez4.z, ez4.w};
-                const unsigned char* I0 = Is(k);
-                const unsigned char* I1 = Is(k - 1);
-                const unsigned char* a0 = I0 + r * Y4_IW + xbi;        // plane k, row r
-                const unsigned char* a1 = I0 + (r - 1) * Y4_IW + xbi;  // plane k, row r-1
-                const unsigned char* b0 = I1 + r * Y4_IW + xbi;        // plane k-1, row r
-                const unsigned char* b1 = I1 + (r - 1) * Y4_IW + xbi;  // plane k-1, row r-1
+                const float4 dx4 = lds4(dxs + Y4_TX + 4 * lane);
+                const float dex[4] = {dx4.x, dx4.y, dx4.z, dx4.w};
+                const unsigned char* I0 = Iw(k);
+                const unsigned char* I1 = Iw(k - 1);
+                const unsigned char* a0 = I0 + r * Y4_IW + T.xbi;        // plane k, row r
+                const unsigned char* a1 = I0 + (r - 1) * Y4_IW + T.xbi;  // plane k, row r-1
+                const unsigned char* b0 = I1 + r * Y4_IW + T.xbi;        // plane k-1, row r
+                const unsigned char* b1 = I1 + (r - 1) * Y4_IW + T.xbi;  // plane k-1, row r-1
                 const unsigned w_a0 = *reinterpret_cast<const unsigned*>(a0), w_a1 = *reinterpret_cast<const unsigned*>(a1);
                 const unsigned w_b0 = *reinterpret_cast<const unsigned*>(b0), w_b1 = *reinterpret_cast<const unsigned*>(b1);
                 const int kk = pz + 1;
-                const float dez = P.den_e[2][kk - 1];
-                const bool upd_all = xb >= 1 && xb + 3 <= P.SX - 2 && py >= 1 && py <= P.SY - 2 &&
-                                     (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
-                const bool no_pml = xb + 1 > P.npml[0][0] && xb + 4 <= P.X - P.npml[0][1] && j > P.npml[1][0] &&
-                                    j < P.Y + 1 - P.npml[1][1] && kk > P.npml[2][0] && kk < P.Z + 1 - P.npml[2][1];
-                const unsigned m = a0[0];
+                // cells whose Ex / Ey / Ez this step updates
+                const bool zxy = P.per[2] || (pz >= 1 && pz <= P.SZ - 2), zz = P.per[2] || pz <= P.SZ - 2;
+                const unsigned mx = zxy ? T.emx : 0u, my = zxy ? T.emy : 0u, mz = zz ? T.emz : 0u;
+                const unsigned m = w_a0 & 0xffu;
                 const unsigned rep = m * 0x01010101u;
+                // one material around every cell; a cell on an index-1 plane
+                // uses material 0 without averaging, so there the group's
+                // material must be 0
                 const bool uniform = w_a0 == rep && w_a1 == rep && w_b0 == rep && w_b1 == rep && a0[-1] == m &&
-                                     a1[-1] == m && b0[-1] == m;
-                float ex_n[4], ey_n[4], ez_n[4];
-                if (upd_all && uniform) {
+                                     a1[-1] == m && b0[-1] == m &&
+                                     (m == 0 || !(T.unavg_xy || (!P.per[2] && kk == 1)));
+                if (!(mx | my | mz)) {
+                } else if (uniform) {
                     const float gax = gab[m * 6 + 0], gay = gab[m * 6 + 1], gaz = gab[m * 6 + 2];
                     const float gbx = gab[m * 6 + 3], gby = gab[m * 6 + 4], gbz = gab[m * 6 + 5];
+                    float ex_n[4], ey_n[4], ez_n[4];
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
-                        const float dex = P.den_e[0][xb + e];
                         ex_n[e] = gax * vex[e] + gbx * ((hz[e] - hzj[e]) * dey + (hyp[e] - hy[e]) * dez);
-                        ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex + (hx[e] - hxp[e]) * dez);
-                        ez_n[e] = gaz * vez[e] + gbz * ((hy[e] - him_y[e]) * dex + (hxj[e] - hx[e]) * dey);
+                        ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex[e] + (hx[e] - hxp[e]) * dez);
+                        ez_n[e] = gaz * vez[e] + gbz * ((hy[e] - him_y[e]) * dex[e] + (hxj[e] - hx[e]) * dey);
                     }
-                    if (!no_pml) {
+                    // CPML terms in the reference's order: Ex (y, z), Ey (x, z), Ez (x, y)
+                    if (T.e_xpml) {
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
-                            ex_n[e] = y4_e_pml(P, 0, xb + e, py, pz, ex_n[e], gbx, hz[e] - hzj[e], hyp[e] - hy[e]);
-                            ey_n[e] = y4_e_pml(P, 1, xb + e, py, pz, ey_n[e], gby, him_z[e] - hz[e], hx[e] - hxp[e]);
-                            ez_n[e] = y4_e_pml(P, 2, xb + e, py, pz, ez_n[e], gbz, hy[e] - him_y[e], hxj[e] - hx[e]);
+                            const float2 t = y4_e_xpml(P, T.xb + e, T.py, pz, him_z[e] - hz[e], hy[e] - him_y[e], gby, gbz,
+                                                       my >> e & 1u, mz >> e & 1u, ey_n[e], ez_n[e]);
+                            ey_n[e] = t.x; ez_n[e] = t.y;
                         }
                     }
-                    const long long c = lin(P, xb, py, pz);
-                    *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[0]) + c) = make_float4(ex_n[0], ex_n[1], ex_n[2], ex_n[3]);
-                    *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[1]) + c) = make_float4(ey_n[0], ey_n[1], ey_n[2], ey_n[3]);
-                    *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[2]) + c) = make_float4(ez_n[0], ez_n[1], ez_n[2], ez_n[3]);
+                    if (T.qye_lo | T.qye_hi) {
+                        float dzy[4], dxy[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) { dzy[e] = hz[e] - hzj[e]; dxy[e] = hxj[e] - hx[e]; }
+                        for (int s = 0; s < 2; s++) {
+                            const int q = s ? T.qye_hi : T.qye_lo;
+                            if (!q) continue;
+                            const int n = P.npml[1][s];
+                            const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
+                            y4_psi_row(P.psi_e[0][1][s], P.psi_e[0][1][s], true, mx, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dzy, gbx, ex_n);
+                            y4_psi_row(P.psi_e[2][1][s], P.psi_e[2][1][s], true, mz, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dxy, gbz, ez_n);
+                        }
+                    }
+                    const int qzl = (kk >= 2 && kk <= P.npml[2][0]) ? kk : 0;
+                    const int qzh = (kk >= P.Z + 1 - P.npml[2][1] && kk <= P.Z - 1) ? P.Z + 1 - kk : 0;
+                    if (qzl | qzh) {
+                        float dyz[4], dxz[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) { dyz[e] = hyp[e] - hy[e]; dxz[e] = hx[e] - hxp[e]; }
+                        for (int s = 0; s < 2; s++) {
+                            const int q = s ? qzh : qzl;
+                            if (!q) continue;
+                            const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
+                            y4_psi_row(P.psi_e[0][2][s], P.psi_e[0][2][s], true, mx, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dyz, gbx, ex_n);
+                            y4_psi_row(P.psi_e[1][2][s], P.psi_e[1][2][s], true, my, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dxz, gby, ey_n);
+                        }
+                    }
+                    const long long c = (long long)pz * P.plane + T.rowoff;
+                    if (mx) y4_store4(P.E2[0], c, mx, ex_n);
+                    if (my) y4_store4(P.E2[1], c, my, ey_n);
+                    if (mz) y4_store4(P.E2[2], c, mz, ez_n);
                 } else {
+                    const int py = T.py;
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
-                        const int px = xb + e, i = px + 1;
+                        const int px = T.xb + e, i = px + 1;
                         if (px >= P.SX) continue;
                         const bool ex_u = px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
                         const bool ey_u = px >= 1 && px <= P.SX - 2 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
@@ -428,11 +655,10 @@ __global__ void __maxnreg__(112) k_yee4(const __grid_constant__ AemParams P) {
                         const int idc = unavg ? 0 : a0[e], idx_ = unavg ? 0 : a0[e - 1], idy_ = unavg ? 0 : a1[e],
                                   idxy = unavg ? 0 : a1[e - 1];
                         const int pdc = unavg ? 0 : b0[e], pdx = unavg ? 0 : b0[e - 1], pdy = unavg ? 0 : b1[e];
-                        const float dex = P.den_e[0][i - 1];
                         const long long c = lin(P, px, py, pz);
                         if (ex_u) stf4(P.E2[0], c, y4_e_comp(P, gab, 0, px, py, pz, vex[e], hz[e] - hzj[e], hyp[e] - hy[e], dey, dez, idc, idy_, pdc, pdy));
-                        if (ey_u) stf4(P.E2[1], c, y4_e_comp(P, gab, 1, px, py, pz, vey[e], him_z[e] - hz[e], hx[e] - hxp[e], dex, dez, idc, idx_, pdc, pdx));
-                        if (ez_u) stf4(P.E2[2], c, y4_e_comp(P, gab, 2, px, py, pz, vez[e], hy[e] - him_y[e], hxj[e] - hx[e], dex, dey, idc, idx_, idy_, idxy));
+                        if (ey_u) stf4(P.E2[1], c, y4_e_comp(P, gab, 1, px, py, pz, vey[e], him_z[e] - hz[e], hx[e] - hxp[e], dex[e], dez, idc, idx_, pdc, pdx));
+                        if (ez_u) stf4(P.E2[2], c, y4_e_comp(P, gab, 2, px, py, pz, vez[e], hy[e] - him_y[e], hxj[e] - hx[e], dex[e], dey, idc, idx_, idy_, idxy));
                     }
                 }
             }
@@ -440,21 +666,62 @@ __global__ void __maxnreg__(112) k_yee4(const __grid_constant__ AemParams P) {
 #pragma unroll
         for (int e = 0; e < 4; e++) { hxp[e] = hx[e]; hyp[e] = hy[e]; }
     }
-    cp_wait0();  // no copy may still target this CTA's shared memory at exit
+}
+
+// ---- host side ----
+
+static PFN_cuTensorMapEncodeTiled_v12000 y4_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// 3-D map over a [SZ][SY][PX] array of `esize`-byte elements, box bx x by x 1
+static void y4_map(CUtensorMap* m, const void* base, CUtensorMapDataType t, int esize, const AemParams& P, int bx, int by) {
+    auto enc = y4_encoder();
+    if (!enc) throw std::runtime_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)P.PX, (cuuint64_t)P.SY, (cuuint64_t)P.SZ};
+    const cuuint64_t strides[2] = {(cuuint64_t)P.PX * esize, (cuuint64_t)P.PX * P.SY * esize};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(m, t, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
 }
 
 int launch_yee4(const AemParams& P, cudaStream_t s) {
     static bool attr_set[64] = {};
+    static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaFuncSetAttribute(k_yee4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y4_SMEM);
-        attr_set[dev] = true;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+            cudaFuncSetAttribute(k_yee4, cudaFuncAttributeMaxDynamicSharedMemorySize, Y4_SMEM);
+            cudaFuncSetAttribute(k_yee4, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            attr_set[dev] = true;
+        }
     }
+    if (!P.err) throw std::runtime_error("fused kernel launched without an error counter");
+    Y4Maps M;
+    for (int c = 0; c < 3; c++) {
+        y4_map(&M.e[c], P.E[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, P, Y4_EW, Y4_ER);
+        y4_map(&M.h[c], P.H[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, P, Y4_HW, Y4_HR);
+    }
+    y4_map(&M.id, P.cell, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, P, Y4_IW, Y4_IR);
     // the last position of a non-periodic axis is never updated: no tile for it
     const int ux = P.SX - 1, uy = P.SY - 1, uz = P.per[2] ? P.SZ : P.SZ - 1;
     dim3 blk(32, Y4_TY + 1), grd((ux + Y4_TX - 1) / Y4_TX, (uy + Y4_TY - 1) / Y4_TY, (uz + Y4_ZC - 1) / Y4_ZC);
-    k_yee4<<<grd, blk, Y4_SMEM, s>>>(P);
+    k_yee4<<<grd, blk, Y4_SMEM, s>>>(P, M);
     return 1;
 }
 
