@@ -43,6 +43,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "aem_dev.cuh"
 #include "aem_kernels.h"
@@ -321,7 +322,9 @@ struct Y4Row {
 
 // H_new of the thread's four cells (row r of the tile) from E0 (plane k),
 // E1 (k+1), Ho (H_old k); non-updated cells keep H_old.  `store`: write to
-// H2 / psi_h2 (owned cells).
+// H2 / psi_h2 (owned cells).  IN: the tile and plane lie inside the update
+// range and outside every CPML slab (no masks, no CPML terms).
+template <bool IN>
 __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, const float* E0, const float* E1,
                                            const float* Ho, int pz, int hzm, float dhz, const float* dxs, float dhy,
                                            bool store, float hx[4], float hy[4], float hz[4]) {
@@ -341,8 +344,8 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
     const float vhx[4] = {h0x.x, h0x.y, h0x.z, h0x.w}, vhy[4] = {h0y.x, h0y.y, h0y.z, h0y.w},
                 vhz[4] = {h0z.x, h0z.y, h0z.z, h0z.w};
     // cells of the group inside the H update range (all four in the bulk)
-    const unsigned mk = pz <= hzm ? T.hmask : 0u;
-    if (!mk) {
+    const unsigned mk = IN ? 0xFu : (pz <= hzm ? T.hmask : 0u);
+    if (!IN && !mk) {
 #pragma unroll
         for (int e = 0; e < 4; e++) { hx[e] = vhx[e]; hy[e] = vhy[e]; hz[e] = vhz[e]; }
         return;
@@ -355,6 +358,15 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
         hx[e] = vhx[e] + DB * ((vez[e] - vezj[e]) * dhy + (veyk[e] - vey[e]) * dhz);
         hy[e] = vhy[e] + DB * ((vezi[e] - vez[e]) * dhx[e] + (vex[e] - vexk[e]) * dhz);
         hz[e] = vhz[e] + DB * ((vey[e] - veyi[e]) * dhx[e] + (vexj[e] - vex[e]) * dhy);
+    }
+    if constexpr (IN) {
+        if (store) {
+            const long long c = (long long)pz * P.plane + T.rowoff;
+            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[0]) + c) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[1]) + c) = make_float4(hy[0], hy[1], hy[2], hy[3]);
+            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.H2[2]) + c) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+        }
+        return;
     }
     // CPML terms in the reference's order: Hx (y, z), Hy (x, z), Hz (x, y)
     if (T.h_xpml) {
@@ -502,6 +514,12 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
     T.qye_hi = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
     const bool yin = T.py >= 0 && T.py < P.SY;
     const float dhy = yin ? P.den_h[1][T.py] : 0.0f, dey = yin ? P.den_e[1][T.py] : 0.0f;
+    // the tile (with its -x / -y halo) inside the update range and outside
+    // the x and y CPML slabs of H and E (reference indices x0..x0+128,
+    // y0..y0+8)
+    const bool tile_in = x0 >= 1 && x0 + Y4_TX - 1 <= P.SX - 2 && x0 > P.npml[0][0] &&
+                         x0 + Y4_TX < P.X + 1 - P.npml[0][1] && y0 >= 1 && y0 + Y4_TY - 1 <= P.SY - 2 &&
+                         y0 > P.npml[1][0] && y0 + Y4_TY < P.Y + 1 - P.npml[1][1];
 
     bool ok = y4_bar_wait(&bar[0], 0);
     if (!__syncthreads_and(ok)) {
@@ -513,7 +531,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
     if (below && T.own) {
         float hz_unused[4];
         const int pzb = zw(z0 - 1);
-        y4_h_group(P, T, Ew(z0 - 1), Ew(z0), Hw(z0 - 1), pzb, hzm, P.den_h[2][pzb], dxs, dhy, false, hxp, hyp, hz_unused);
+        y4_h_group<false>(P, T, Ew(z0 - 1), Ew(z0), Hw(z0 - 1), pzb, hzm, P.den_h[2][pzb], dxs, dhy, false, hxp, hyp, hz_unused);
     }
 
     for (int k = z0; k < z1; k++) {
@@ -535,134 +553,154 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
             issue(nullptr, Hw(t), Iw(t), zw(t), b);
         }
 
-        // ---- H_new(k): own rows, the -y halo row (warp 8), the -x halo cell (lane 0)
-        const float* E0 = Ew(k);
-        const float dhz = dzs[k - z0], dez = dzs[Y4_ZC + k - z0];
+        // the plane's update: IN (tile and plane inside the update range and
+        // outside every CPML slab) drops the masks and CPML terms
         float hx[4], hy[4], hz[4];
-        if (T.hrow)
-            y4_h_group(P, T, E0, Ew(k + 1), Hw(k), pz, hzm, dhz, dxs, dhy, T.own, hx, hy, hz);
-        else
-            for (int e = 0; e < 4; e++) hx[e] = hy[e] = hz[e] = 0.0f;
-        float hy_xh = 0.0f, hz_xh = 0.0f;
-        if (lane == 0 && T.own) {
-            const int kz = pz + 1;
-            const bool cpml_yz = (T.qyh_lo | T.qyh_hi) || kz <= P.npml[2][0] - 1 || kz >= P.Z + 1 - P.npml[2][1];
-            const float2 hh = y4_h_xhalo(P, E0, Ew(k + 1), Hw(k), T.r, x0, T.py, pz, hzm, cpml_yz, dxs[2 * Y4_TX], dhy, dhz);
-            hy_xh = hh.x; hz_xh = hh.y;
-        }
-        *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
-        *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
-        __syncthreads();
+        auto plane = [&](auto in_tag) {
+            constexpr bool IN = decltype(in_tag)::value;
+            // ---- H_new(k): own rows, the -y halo row (warp 8), the -x halo cell (lane 0)
+            const float* E0 = Ew(k);
+            const float dhz = dzs[k - z0], dez = dzs[Y4_ZC + k - z0];
+            if (T.hrow)
+                y4_h_group<IN>(P, T, E0, Ew(k + 1), Hw(k), pz, hzm, dhz, dxs, dhy, T.own, hx, hy, hz);
+            else
+                for (int e = 0; e < 4; e++) hx[e] = hy[e] = hz[e] = 0.0f;
+            float hy_xh = 0.0f, hz_xh = 0.0f;
+            if (lane == 0 && T.own) {
+                const int kz = pz + 1;
+                const bool cpml_yz = !IN && ((T.qyh_lo | T.qyh_hi) || kz <= P.npml[2][0] - 1 || kz >= P.Z + 1 - P.npml[2][1]);
+                const float2 hh = y4_h_xhalo(P, E0, Ew(k + 1), Hw(k), T.r, x0, T.py, pz, hzm, cpml_yz, dxs[2 * Y4_TX], dhy, dhz);
+                hy_xh = hh.x; hz_xh = hh.y;
+            }
+            *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+            *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+            __syncthreads();
 
-        // ---- E_new(k) of the own rows
-        if (w < Y4_TY) {
-            float hz_im0 = __shfl_up_sync(FULL, hz[3], 1), hy_im0 = __shfl_up_sync(FULL, hy[3], 1);
-            if (lane == 0) { hz_im0 = hz_xh; hy_im0 = hy_xh; }
-            if (T.own) {
-                const int r = T.r;
-                const float4 hxj4 = lds4(Hn + (0 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
-                const float4 hzj4 = lds4(Hn + (1 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
-                const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
-                const float him_z[4] = {hz_im0, hz[0], hz[1], hz[2]}, him_y[4] = {hy_im0, hy[0], hy[1], hy[2]};
-                const float4 ex4 = lds4(E0 + 0 * Y4_EC + r * Y4_EW + T.xi), ey4 = lds4(E0 + 1 * Y4_EC + r * Y4_EW + T.xi),
-                             ez4 = lds4(E0 + 2 * Y4_EC + r * Y4_EW + T.xi);
-                const float vex[4] = {ex4.x, ex4.y, ex4.z, ex4.w}, vey[4] = {ey4.x, ey4.y, ey4.z, ey4.w},
-                            vez[4] = {ez4.x, ez4.y, ez4.z, ez4.w};
-                const float4 dx4 = lds4(dxs + Y4_TX + 4 * lane);
-                const float dex[4] = {dx4.x, dx4.y, dx4.z, dx4.w};
-                const unsigned char* I0 = Iw(k);
-                const unsigned char* I1 = Iw(k - 1);
-                const unsigned char* a0 = I0 + r * Y4_IW + T.xbi;        // plane k, row r
-                const unsigned char* a1 = I0 + (r - 1) * Y4_IW + T.xbi;  // plane k, row r-1
-                const unsigned char* b0 = I1 + r * Y4_IW + T.xbi;        // plane k-1, row r
-                const unsigned char* b1 = I1 + (r - 1) * Y4_IW + T.xbi;  // plane k-1, row r-1
-                const unsigned w_a0 = *reinterpret_cast<const unsigned*>(a0), w_a1 = *reinterpret_cast<const unsigned*>(a1);
-                const unsigned w_b0 = *reinterpret_cast<const unsigned*>(b0), w_b1 = *reinterpret_cast<const unsigned*>(b1);
-                const int kk = pz + 1;
-                // cells whose Ex / Ey / Ez this step updates
-                const bool zxy = P.per[2] || (pz >= 1 && pz <= P.SZ - 2), zz = P.per[2] || pz <= P.SZ - 2;
-                const unsigned mx = zxy ? T.emx : 0u, my = zxy ? T.emy : 0u, mz = zz ? T.emz : 0u;
-                const unsigned m = w_a0 & 0xffu;
-                const unsigned rep = m * 0x01010101u;
-                // one material around every cell; a cell on an index-1 plane
-                // uses material 0 without averaging, so there the group's
-                // material must be 0
-                const bool uniform = w_a0 == rep && w_a1 == rep && w_b0 == rep && w_b1 == rep && a0[-1] == m &&
-                                     a1[-1] == m && b0[-1] == m &&
-                                     (m == 0 || !(T.unavg_xy || (!P.per[2] && kk == 1)));
-                if (!(mx | my | mz)) {
-                } else if (uniform) {
-                    const float gax = gab[m * 6 + 0], gay = gab[m * 6 + 1], gaz = gab[m * 6 + 2];
-                    const float gbx = gab[m * 6 + 3], gby = gab[m * 6 + 4], gbz = gab[m * 6 + 5];
-                    float ex_n[4], ey_n[4], ez_n[4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        ex_n[e] = gax * vex[e] + gbx * ((hz[e] - hzj[e]) * dey + (hyp[e] - hy[e]) * dez);
-                        ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex[e] + (hx[e] - hxp[e]) * dez);
-                        ez_n[e] = gaz * vez[e] + gbz * ((hy[e] - him_y[e]) * dex[e] + (hxj[e] - hx[e]) * dey);
-                    }
-                    // CPML terms in the reference's order: Ex (y, z), Ey (x, z), Ez (x, y)
-                    if (T.e_xpml) {
-#pragma unroll
+            // ---- E_new(k) of the own rows
+            if (w < Y4_TY) {
+                float hz_im0 = __shfl_up_sync(FULL, hz[3], 1), hy_im0 = __shfl_up_sync(FULL, hy[3], 1);
+                if (lane == 0) { hz_im0 = hz_xh; hy_im0 = hy_xh; }
+                if (T.own) {
+                    const int r = T.r;
+                    const float4 hxj4 = lds4(Hn + (0 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
+                    const float4 hzj4 = lds4(Hn + (1 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
+                    const float hxj[4] = {hxj4.x, hxj4.y, hxj4.z, hxj4.w}, hzj[4] = {hzj4.x, hzj4.y, hzj4.z, hzj4.w};
+                    const float him_z[4] = {hz_im0, hz[0], hz[1], hz[2]}, him_y[4] = {hy_im0, hy[0], hy[1], hy[2]};
+                    const float4 ex4 = lds4(E0 + 0 * Y4_EC + r * Y4_EW + T.xi), ey4 = lds4(E0 + 1 * Y4_EC + r * Y4_EW + T.xi),
+                                 ez4 = lds4(E0 + 2 * Y4_EC + r * Y4_EW + T.xi);
+                    const float vex[4] = {ex4.x, ex4.y, ex4.z, ex4.w}, vey[4] = {ey4.x, ey4.y, ey4.z, ey4.w},
+                                vez[4] = {ez4.x, ez4.y, ez4.z, ez4.w};
+                    const float4 dx4 = lds4(dxs + Y4_TX + 4 * lane);
+                    const float dex[4] = {dx4.x, dx4.y, dx4.z, dx4.w};
+                    const unsigned char* I0 = Iw(k);
+                    const unsigned char* I1 = Iw(k - 1);
+                    const unsigned char* a0 = I0 + r * Y4_IW + T.xbi;        // plane k, row r
+                    const unsigned char* a1 = I0 + (r - 1) * Y4_IW + T.xbi;  // plane k, row r-1
+                    const unsigned char* b0 = I1 + r * Y4_IW + T.xbi;        // plane k-1, row r
+                    const unsigned char* b1 = I1 + (r - 1) * Y4_IW + T.xbi;  // plane k-1, row r-1
+                    const unsigned w_a0 = *reinterpret_cast<const unsigned*>(a0), w_a1 = *reinterpret_cast<const unsigned*>(a1);
+                    const unsigned w_b0 = *reinterpret_cast<const unsigned*>(b0), w_b1 = *reinterpret_cast<const unsigned*>(b1);
+                    const int kk = pz + 1;
+                    // cells whose Ex / Ey / Ez this step updates
+                    const bool zxy = P.per[2] || (pz >= 1 && pz <= P.SZ - 2), zz = P.per[2] || pz <= P.SZ - 2;
+                    const unsigned mx = IN ? 0xFu : zxy ? T.emx : 0u, my = IN ? 0xFu : zxy ? T.emy : 0u,
+                                   mz = IN ? 0xFu : zz ? T.emz : 0u;
+                    const unsigned m = w_a0 & 0xffu;
+                    const unsigned rep = m * 0x01010101u;
+                    // one material around every cell; a cell on an index-1 plane
+                    // uses material 0 without averaging, so there the group's
+                    // material must be 0
+                    const bool uniform = w_a0 == rep && w_a1 == rep && w_b0 == rep && w_b1 == rep && a0[-1] == m &&
+                                         a1[-1] == m && b0[-1] == m &&
+                                         (IN || m == 0 || !(T.unavg_xy || (!P.per[2] && kk == 1)));
+                    if (!IN && !(mx | my | mz)) {
+                    } else if (uniform) {
+                        const float gax = gab[m * 6 + 0], gay = gab[m * 6 + 1], gaz = gab[m * 6 + 2];
+                        const float gbx = gab[m * 6 + 3], gby = gab[m * 6 + 4], gbz = gab[m * 6 + 5];
+                        float ex_n[4], ey_n[4], ez_n[4];
+    #pragma unroll
                         for (int e = 0; e < 4; e++) {
-                            const float2 t = y4_e_xpml(P, T.xb + e, T.py, pz, him_z[e] - hz[e], hy[e] - him_y[e], gby, gbz,
-                                                       my >> e & 1u, mz >> e & 1u, ey_n[e], ez_n[e]);
-                            ey_n[e] = t.x; ez_n[e] = t.y;
+                            ex_n[e] = gax * vex[e] + gbx * ((hz[e] - hzj[e]) * dey + (hyp[e] - hy[e]) * dez);
+                            ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex[e] + (hx[e] - hxp[e]) * dez);
+                            ez_n[e] = gaz * vez[e] + gbz * ((hy[e] - him_y[e]) * dex[e] + (hxj[e] - hx[e]) * dey);
                         }
-                    }
-                    if (T.qye_lo | T.qye_hi) {
-                        float dzy[4], dxy[4];
-#pragma unroll
-                        for (int e = 0; e < 4; e++) { dzy[e] = hz[e] - hzj[e]; dxy[e] = hxj[e] - hx[e]; }
-                        for (int s = 0; s < 2; s++) {
-                            const int q = s ? T.qye_hi : T.qye_lo;
-                            if (!q) continue;
-                            const int n = P.npml[1][s];
-                            const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
-                            y4_psi_row(P.psi_e[0][1][s], P.psi_e[0][1][s], true, mx, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dzy, gbx, ex_n);
-                            y4_psi_row(P.psi_e[2][1][s], P.psi_e[2][1][s], true, mz, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dxy, gbz, ez_n);
+                        if constexpr (IN) {
+                            const long long c = (long long)pz * P.plane + T.rowoff;
+                            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[0]) + c) = make_float4(ex_n[0], ex_n[1], ex_n[2], ex_n[3]);
+                            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[1]) + c) = make_float4(ey_n[0], ey_n[1], ey_n[2], ey_n[3]);
+                            *reinterpret_cast<float4*>(reinterpret_cast<float*>(P.E2[2]) + c) = make_float4(ez_n[0], ez_n[1], ez_n[2], ez_n[3]);
+                            return;
                         }
-                    }
-                    const int qzl = (kk >= 2 && kk <= P.npml[2][0]) ? kk : 0;
-                    const int qzh = (kk >= P.Z + 1 - P.npml[2][1] && kk <= P.Z - 1) ? P.Z + 1 - kk : 0;
-                    if (qzl | qzh) {
-                        float dyz[4], dxz[4];
-#pragma unroll
-                        for (int e = 0; e < 4; e++) { dyz[e] = hyp[e] - hy[e]; dxz[e] = hx[e] - hxp[e]; }
-                        for (int s = 0; s < 2; s++) {
-                            const int q = s ? qzh : qzl;
-                            if (!q) continue;
-                            const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
-                            y4_psi_row(P.psi_e[0][2][s], P.psi_e[0][2][s], true, mx, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dyz, gbx, ex_n);
-                            y4_psi_row(P.psi_e[1][2][s], P.psi_e[1][2][s], true, my, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dxz, gby, ey_n);
+                        // CPML terms in the reference's order: Ex (y, z), Ey (x, z), Ez (x, y)
+                        if (T.e_xpml) {
+    #pragma unroll
+                            for (int e = 0; e < 4; e++) {
+                                const float2 t = y4_e_xpml(P, T.xb + e, T.py, pz, him_z[e] - hz[e], hy[e] - him_y[e], gby, gbz,
+                                                           my >> e & 1u, mz >> e & 1u, ey_n[e], ez_n[e]);
+                                ey_n[e] = t.x; ez_n[e] = t.y;
+                            }
                         }
-                    }
-                    const long long c = (long long)pz * P.plane + T.rowoff;
-                    if (mx) y4_store4(P.E2[0], c, mx, ex_n);
-                    if (my) y4_store4(P.E2[1], c, my, ey_n);
-                    if (mz) y4_store4(P.E2[2], c, mz, ez_n);
-                } else {
-                    const int py = T.py;
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int px = T.xb + e, i = px + 1;
-                        if (px >= P.SX) continue;
-                        const bool ex_u = px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
-                        const bool ey_u = px >= 1 && px <= P.SX - 2 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
-                        const bool ez_u = px >= 1 && px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || pz <= P.SZ - 2);
-                        if (!(ex_u || ey_u || ez_u)) continue;
-                        const bool unavg = i == 1 || j == 1 || (!P.per[2] && kk == 1);
-                        const int idc = unavg ? 0 : a0[e], idx_ = unavg ? 0 : a0[e - 1], idy_ = unavg ? 0 : a1[e],
-                                  idxy = unavg ? 0 : a1[e - 1];
-                        const int pdc = unavg ? 0 : b0[e], pdx = unavg ? 0 : b0[e - 1], pdy = unavg ? 0 : b1[e];
-                        const long long c = lin(P, px, py, pz);
-                        if (ex_u) stf4(P.E2[0], c, y4_e_comp(P, gab, 0, px, py, pz, vex[e], hz[e] - hzj[e], hyp[e] - hy[e], dey, dez, idc, idy_, pdc, pdy));
-                        if (ey_u) stf4(P.E2[1], c, y4_e_comp(P, gab, 1, px, py, pz, vey[e], him_z[e] - hz[e], hx[e] - hxp[e], dex[e], dez, idc, idx_, pdc, pdx));
-                        if (ez_u) stf4(P.E2[2], c, y4_e_comp(P, gab, 2, px, py, pz, vez[e], hy[e] - him_y[e], hxj[e] - hx[e], dex[e], dey, idc, idx_, idy_, idxy));
+                        if (T.qye_lo | T.qye_hi) {
+                            float dzy[4], dxy[4];
+    #pragma unroll
+                            for (int e = 0; e < 4; e++) { dzy[e] = hz[e] - hzj[e]; dxy[e] = hxj[e] - hx[e]; }
+                            for (int s = 0; s < 2; s++) {
+                                const int q = s ? T.qye_hi : T.qye_lo;
+                                if (!q) continue;
+                                const int n = P.npml[1][s];
+                                const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
+                                y4_psi_row(P.psi_e[0][1][s], P.psi_e[0][1][s], true, mx, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dzy, gbx, ex_n);
+                                y4_psi_row(P.psi_e[2][1][s], P.psi_e[2][1][s], true, mz, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dxy, gbz, ez_n);
+                            }
+                        }
+                        const int qzl = (kk >= 2 && kk <= P.npml[2][0]) ? kk : 0;
+                        const int qzh = (kk >= P.Z + 1 - P.npml[2][1] && kk <= P.Z - 1) ? P.Z + 1 - kk : 0;
+                        if (qzl | qzh) {
+                            float dyz[4], dxz[4];
+    #pragma unroll
+                            for (int e = 0; e < 4; e++) { dyz[e] = hyp[e] - hy[e]; dxz[e] = hx[e] - hxp[e]; }
+                            for (int s = 0; s < 2; s++) {
+                                const int q = s ? qzh : qzl;
+                                if (!q) continue;
+                                const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
+                                y4_psi_row(P.psi_e[0][2][s], P.psi_e[0][2][s], true, mx, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dyz, gbx, ex_n);
+                                y4_psi_row(P.psi_e[1][2][s], P.psi_e[1][2][s], true, my, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dxz, gby, ey_n);
+                            }
+                        }
+                        const long long c = (long long)pz * P.plane + T.rowoff;
+                        if (mx) y4_store4(P.E2[0], c, mx, ex_n);
+                        if (my) y4_store4(P.E2[1], c, my, ey_n);
+                        if (mz) y4_store4(P.E2[2], c, mz, ez_n);
+                    } else {
+                        const int py = T.py;
+    #pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            const int px = T.xb + e, i = px + 1;
+                            if (px >= P.SX) continue;
+                            const bool ex_u = px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
+                            const bool ey_u = px >= 1 && px <= P.SX - 2 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
+                            const bool ez_u = px >= 1 && px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || pz <= P.SZ - 2);
+                            if (!(ex_u || ey_u || ez_u)) continue;
+                            const bool unavg = i == 1 || j == 1 || (!P.per[2] && kk == 1);
+                            const int idc = unavg ? 0 : a0[e], idx_ = unavg ? 0 : a0[e - 1], idy_ = unavg ? 0 : a1[e],
+                                      idxy = unavg ? 0 : a1[e - 1];
+                            const int pdc = unavg ? 0 : b0[e], pdx = unavg ? 0 : b0[e - 1], pdy = unavg ? 0 : b1[e];
+                            const long long c = lin(P, px, py, pz);
+                            if (ex_u) stf4(P.E2[0], c, y4_e_comp(P, gab, 0, px, py, pz, vex[e], hz[e] - hzj[e], hyp[e] - hy[e], dey, dez, idc, idy_, pdc, pdy));
+                            if (ey_u) stf4(P.E2[1], c, y4_e_comp(P, gab, 1, px, py, pz, vey[e], him_z[e] - hz[e], hx[e] - hxp[e], dex[e], dez, idc, idx_, pdc, pdx));
+                            if (ez_u) stf4(P.E2[2], c, y4_e_comp(P, gab, 2, px, py, pz, vez[e], hy[e] - him_y[e], hxj[e] - hx[e], dex[e], dey, idc, idx_, idy_, idxy));
+                        }
                     }
                 }
             }
-        }
+        };
+        const int kz = pz + 1;
+        const bool plane_in = (P.per[2] || (pz >= 1 && pz <= P.SZ - 2)) && pz <= hzm && kz > P.npml[2][0] &&
+                              kz < P.Z + 1 - P.npml[2][1];
+        if (tile_in && plane_in)
+            plane(std::true_type{});
+        else
+            plane(std::false_type{});
 #pragma unroll
         for (int e = 0; e < 4; e++) { hxp[e] = hx[e]; hyp[e] = hy[e]; }
     }
