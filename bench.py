@@ -70,15 +70,18 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def dram_traffic_per_cell():
-    """Per-cell-update DRAM bytes of the Yee update from the committed ncu
-    summary (profiles/yee_update_dipole_ellipsoids.md, line
-    'dram_bytes_per_cell_update: X'), or None."""
+def dram_traffic_ratio():
+    """Measured DRAM bytes of one fused Yee launch over its algorithmic bytes,
+    from the committed ncu summary (profiles/yee_update_dipole_ellipsoids.md,
+    line 'dram_traffic_over_algorithmic: X'), or None.  The capture runs a
+    smaller instance of the workload; the ratio (halo re-reads of the tiles)
+    carries over to the full grid, the per-cell bytes do not (the CPML share
+    of the cells shrinks as the grid grows)."""
     p = os.path.join(ROOT, "profiles", "yee_update_dipole_ellipsoids.md")
     try:
         with open(p) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_cell_update:"):
+                if line.startswith("dram_traffic_over_algorithmic:"):
                     return float(line.split(":", 1)[1])
     except OSError:
         pass
@@ -251,11 +254,11 @@ def ours(args):
     t_yee = (prof["update_h"][0] + prof["update_e"][0] + prof["yee"][0]) / K / 1e3
     peak, peak_kind = hbm_peak()
     achieved = bytes_step / t_yee / 1e9
-    tpc = dram_traffic_per_cell()
+    ratio = dram_traffic_ratio()
     kname = "k_yee (fused H+E step)" if prof["yee"][1] else "k_update_h + k_update_e (one Yee step)"
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": round(tpc * cells) if tpc else None,
+                "traffic": round(ratio * bytes_step) if ratio else None,
                 "algorithmic_bytes": round(bytes_step), "bytes_per_cell_update": round(bytes_step / cells, 2)}
     phases = {k: round(v[0] / K, 4) for k, v in prof.items() if v[1]}
     sim.close()
