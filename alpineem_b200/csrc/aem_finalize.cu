@@ -4,6 +4,7 @@
 // The .dat file keeps the reference's line numbers and whitespace token
 // columns (what utility_scripts/post_processor*.py parse); numbers use one
 // fixed format (reals "%.9E", integers "%12d").
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -127,6 +128,10 @@ void Solver::finalize_and_write() {
     if (nff > 0) {
         const size_t L = FF_.len;
         std::vector<cplx> uw = fetch(FF_.UW, 6 * (size_t)nff * L, K, stream_, d2h_bytes_);
+        for (int i = 0; i < nff && i < (int)ff_canon_.size(); i++)
+            if (ff_canon_[i] != i)
+                for (int comp = 0; comp < 6; comp++)
+                    std::copy_n(uw.begin() + ((size_t)comp * nff + ff_canon_[i]) * L, L, uw.begin() + ((size_t)comp * nff + i) * L);
         const float eta = std::sqrt(mu0 / ep0);
         for (int i = 0; i < nff; i++) {
             const float a1 = d.ff_theta[i], a2 = d.ff_phi[i];

@@ -12,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <stdexcept>
+#include <string>
 
 namespace aem {
 
@@ -461,6 +463,21 @@ void Solver::setup_farfield() {
             }
         }
     }
+    // angles of one direction (the poles theta = 0, 180 at every phi) have the
+    // same delays on every face and pass, so the same bins of the Cartesian
+    // components: the batched path bins the first such angle and the others
+    // copy its bins when the output is written
+    ff_canon_.resize(F.nang);
+    {
+        std::map<std::string, int> first;
+        const size_t per = (size_t)3 * 2 * 3;
+        for (int q = 0; q < F.nang; q++) {
+            std::string key;
+            for (int pass = 0; pass <= F.mirror; pass++)
+                key.append(reinterpret_cast<const char*>(&kf[(size_t)(q + pass * F.nang) * per]), per * sizeof(float));
+            ff_canon_[q] = first.emplace(key, q).first->second;
+        }
+    }
     // time batching on the FP32 path when the histograms fit in shared memory
     F.hspan = (int)std::ceil(span) + FF_TB + 8;
     const size_t smem_max = 96 * 1024;
@@ -477,6 +494,7 @@ void Solver::setup_farfield() {
             const int a = f >> 1, s = f & 1;
             std::vector<int> cu, cv;
             for (int va = 0; va < F.nvang; va++) {
+                if (ff_canon_[va % F.nang] != va % F.nang) continue;  // binned by its first angle
                 const float* k = &kf[(((size_t)va * 3 + a) * 2 + s) * 3];
                 (std::fabs(k[1]) <= std::fabs(k[2]) ? cu : cv).push_back(va);
             }
@@ -499,6 +517,8 @@ void Solver::setup_farfield() {
         F.tile0[0] = 0;
         for (int f = 0; f < 6; f++) F.tile0[f + 1] = F.tile0[f] + (long long)F.tiles_u[f >> 1] * F.tiles_v[f >> 1];
         ff_batch_prepare();
+    } else {
+        for (int q = 0; q < F.nang; q++) ff_canon_[q] = q;  // the per-step path bins every angle
     }
     for (int a = 0; a < 3; a++)
         for (int s = 0; s < 2; s++)

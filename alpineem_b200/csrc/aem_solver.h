@@ -102,6 +102,9 @@ class Solver {
     bool split_ = false;  // bulk / port / CPML passes (a port inside a CPML slab)
     AemParams split_params_[2];
     int ff_n0_ = 1;  // first step held in the far-field difference buffer
+    // far-field angle whose bins angle q copies (q itself unless q is a
+    // second angle of the same direction, e.g. a pole at another phi)
+    std::vector<int> ff_canon_;
     long long launches_ = 0;
     size_t h2d_bytes_ = 0, d2h_bytes_ = 0;
     struct ProfMark {
