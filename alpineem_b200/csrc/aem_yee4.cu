@@ -133,31 +133,45 @@ __device__ inline float psi4(const void* rd, void* wr, bool store, float b, floa
     return nw;
 }
 
-// one CPML term over four x-contiguous cells (y or z slab: same depth for
-// all four): psi = b psi + c diff / dl (psi from rd; to wr when store, for
-// the cells of mask mk); f += g psi, lane by lane.  The caller passes a
-// non-empty mask only for groups with an updated cell, whose 16 bytes lie
-// inside the psi row (x < pitch).
-__device__ __forceinline__ void y4_psi_row(const void* rd, void* wr, bool store, unsigned mk, float b, float c, float dl,
-                                           long long q, const float d[4], float g, float f[4]) {
-    if (!mk) return;
-    const float4 o = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(rd) + q);
-    const float ov[4] = {o.x, o.y, o.z, o.w};
-    float nw[4];
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        nw[e] = b * ov[e] + cpml_div(c * d[e], dl);
-        f[e] = f[e] + g * nw[e];
-    }
-    if (!store) return;
-    float* w = reinterpret_cast<float*>(wr) + q;
+// store the cells of mask mk of 4 consecutive floats at base + q
+__device__ __forceinline__ void y4_store4_f(void* base, long long q, unsigned mk, const float v[4]) {
+    float* w = reinterpret_cast<float*>(base) + q;
     if (mk == 0xFu) {
-        *reinterpret_cast<float4*>(w) = make_float4(nw[0], nw[1], nw[2], nw[3]);
+        *reinterpret_cast<float4*>(w) = make_float4(v[0], v[1], v[2], v[3]);
     } else {
 #pragma unroll
         for (int e = 0; e < 4; e++)
-            if (mk >> e & 1u) w[e] = nw[e];
+            if (mk >> e & 1u) w[e] = v[e];
     }
+}
+
+// two CPML terms of one slab over four x-contiguous cells (same depth q,
+// same b, c): both psi rows are loaded before either is used, so the two
+// loads overlap (the arrays may alias as far as the compiler knows)
+__device__ __forceinline__ void y4_psi_row2(const void* rdA, void* wrA, unsigned mkA, const float dA[4], float gA,
+                                            float fA[4], const void* rdB, void* wrB, unsigned mkB, const float dB[4],
+                                            float gB, float fB[4], bool store, float b, float c, float dl, long long q) {
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 oA = mkA ? *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(rdA) + q) : z4;
+    const float4 oB = mkB ? *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(rdB) + q) : z4;
+    const float va[4] = {oA.x, oA.y, oA.z, oA.w}, vb[4] = {oB.x, oB.y, oB.z, oB.w};
+    float na[4], nb[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        na[e] = b * va[e] + cpml_div(c * dA[e], dl);
+        nb[e] = b * vb[e] + cpml_div(c * dB[e], dl);
+    }
+    if (mkA) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) fA[e] = fA[e] + gA * na[e];
+    }
+    if (mkB) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) fB[e] = fB[e] + gB * nb[e];
+    }
+    if (!store) return;
+    if (mkA) y4_store4_f(wrA, q, mkA, na);
+    if (mkB) y4_store4_f(wrB, q, mkB, nb);
 }
 
 // store the cells of mask mk of a 4-cell group (16 bytes when all four)
@@ -201,44 +215,88 @@ __device__ __forceinline__ float3 y4_h_cell(const AemParams& P, int px, int py, 
     return make_float3(hxv, hyv, hzv);
 }
 
-// x-slab CPML terms of one H cell (Hy, Hz), added before the y and z terms
-__device__ __forceinline__ float2 y4_h_xpml(const AemParams& P, int px, int py, int pz, float dzx, float dyx, bool store,
-                                         float hyv, float hzv) {
-    // dzx = ez_ip - ez, dyx = ey - ey_ip
-    const int i = px + 1;
+// x-slab CPML terms of the four cells xb..xb+3 of one H row (Hy, Hz; low
+// slab before high slab), added before the y and z terms.  All psi loads are
+// issued before any is used.  dzx = ez_ip - ez, dyx = ey - ey_ip; cells
+// outside mask mk are left alone.
+__device__ __forceinline__ void y4_h_xpml4(const AemParams& P, int xb, int py, int pz, unsigned mk, const float dzx[4],
+                                           const float dyx[4], bool store, float hy[4], float hz[4]) {
     const float DB = P.DB;
-    const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
-    if (qx_lo) {
-        const long long q = psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]);
-        hyv = hyv + DB * psi4(P.psi_h[1][0][0], P.psi_h2[1][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dzx, P.del[0], q);
-        hzv = hzv + DB * psi4(P.psi_h[2][0][0], P.psi_h2[2][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], dyx, P.del[0], q);
+    int q[2][4];
+    long long idx[2][4];
+    float oy[2][4], oz[2][4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int i = xb + e + 1;
+        q[0][e] = (mk >> e & 1u) && i <= P.npml[0][0] - 1 ? i : 0;
+        q[1][e] = (mk >> e & 1u) && i >= P.X + 1 - P.npml[0][1] ? P.X - i : 0;
     }
-    if (qx_hi) {
-        const long long q = psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]);
-        hyv = hyv + DB * psi4(P.psi_h[1][0][1], P.psi_h2[1][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dzx, P.del[0], q);
-        hzv = hzv + DB * psi4(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], dyx, P.del[0], q);
-    }
-    return make_float2(hyv, hzv);
+#pragma unroll
+    for (int sd = 0; sd < 2; sd++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            idx[sd][e] = q[sd][e] ? psi_idx(P, 0, q[sd][e], xb + e, py, pz, P.npml[0][sd]) : 0;
+            oy[sd][e] = q[sd][e] ? ldf4(P.psi_h[1][0][sd], idx[sd][e]) : 0.0f;
+            oz[sd][e] = q[sd][e] ? ldf4(P.psi_h[2][0][sd], idx[sd][e]) : 0.0f;
+        }
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+#pragma unroll
+        for (int sd = 0; sd < 2; sd++) {
+            if (!q[sd][e]) continue;
+            const float b = P.bh[0][sd][q[sd][e] - 1], c = P.ch[0][sd][q[sd][e] - 1];
+            const float ny = b * oy[sd][e] + cpml_div(c * dzx[e], P.del[0]);
+            const float nz = b * oz[sd][e] + cpml_div(c * dyx[e], P.del[0]);
+            hy[e] = hy[e] + DB * ny;
+            hz[e] = hz[e] + DB * nz;
+            if (store) {
+                stf4(P.psi_h2[1][0][sd], idx[sd][e], ny);
+                stf4(P.psi_h2[2][0][sd], idx[sd][e], nz);
+            }
+        }
 }
 
-// x-slab CPML terms of one E cell (Ey, Ez), added before the y and z terms;
-// psi of a component that is not updated (uy / uz false) is left alone
-__device__ __forceinline__ float2 y4_e_xpml(const AemParams& P, int px, int py, int pz, float dzx, float dyx, float gby,
-                                            float gbz, bool uy, bool uz, float eyv, float ezv) {
-    // dzx = hz(i-1) - hz (Ey), dyx = hy - hy(i-1) (Ez)
-    const int i = px + 1;
-    const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
-    if (qxl) {
-        const long long q = psi_idx(P, 0, qxl, px, py, pz, P.npml[0][0]);
-        if (uy) eyv = eyv + gby * psi4(P.psi_e[1][0][0], P.psi_e[1][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], dzx, P.del[0], q);
-        if (uz) ezv = ezv + gbz * psi4(P.psi_e[2][0][0], P.psi_e[2][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], dyx, P.del[0], q);
+// x-slab CPML terms of the four cells of one E row (Ey for the cells of my,
+// Ez for those of mz; low slab before high slab), added before the y and z
+// terms; all psi loads first.  dzx = hz(i-1) - hz, dyx = hy - hy(i-1).
+__device__ __forceinline__ void y4_e_xpml4(const AemParams& P, int xb, int py, int pz, unsigned my, unsigned mz,
+                                           const float dzx[4], const float dyx[4], float gby, float gbz, float ey[4],
+                                           float ez[4]) {
+    int q[2][4];
+    long long idx[2][4];
+    float oy[2][4], oz[2][4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int i = xb + e + 1;
+        const bool any = (my | mz) >> e & 1u;
+        q[0][e] = any && i >= 2 && i <= P.npml[0][0] ? i : 0;
+        q[1][e] = any && i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1 ? P.X + 1 - i : 0;
     }
-    if (qxh) {
-        const long long q = psi_idx(P, 0, qxh, px, py, pz, P.npml[0][1]);
-        if (uy) eyv = eyv + gby * psi4(P.psi_e[1][0][1], P.psi_e[1][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], dzx, P.del[0], q);
-        if (uz) ezv = ezv + gbz * psi4(P.psi_e[2][0][1], P.psi_e[2][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], dyx, P.del[0], q);
-    }
-    return make_float2(eyv, ezv);
+#pragma unroll
+    for (int sd = 0; sd < 2; sd++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            idx[sd][e] = q[sd][e] ? psi_idx(P, 0, q[sd][e], xb + e, py, pz, P.npml[0][sd]) : 0;
+            oy[sd][e] = q[sd][e] && (my >> e & 1u) ? ldf4(P.psi_e[1][0][sd], idx[sd][e]) : 0.0f;
+            oz[sd][e] = q[sd][e] && (mz >> e & 1u) ? ldf4(P.psi_e[2][0][sd], idx[sd][e]) : 0.0f;
+        }
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+#pragma unroll
+        for (int sd = 0; sd < 2; sd++) {
+            if (!q[sd][e]) continue;
+            const float b = P.be[0][sd][q[sd][e] - 1], c = P.ce[0][sd][q[sd][e] - 1];
+            if (my >> e & 1u) {
+                const float ny = b * oy[sd][e] + cpml_div(c * dzx[e], P.del[0]);
+                ey[e] = ey[e] + gby * ny;
+                stf4(P.psi_e[1][0][sd], idx[sd][e], ny);
+            }
+            if (mz >> e & 1u) {
+                const float nz = b * oz[sd][e] + cpml_div(c * dyx[e], P.del[0]);
+                ez[e] = ez[e] + gbz * nz;
+                stf4(P.psi_e[2][0][sd], idx[sd][e], nz);
+            }
+        }
 }
 
 __device__ inline void y4_gagb(const AemParams& P, const float* gab, int c, int i0, int i1, int i2, int i3, float& ga,
@@ -370,12 +428,10 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
     }
     // CPML terms in the reference's order: Hx (y, z), Hy (x, z), Hz (x, y)
     if (T.h_xpml) {
+        float dzx[4], dyx[4];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            if (!(mk >> e & 1u)) continue;
-            const float2 t = y4_h_xpml(P, T.xb + e, T.py, pz, vezi[e] - vez[e], vey[e] - veyi[e], store, hy[e], hz[e]);
-            hy[e] = t.x; hz[e] = t.y;
-        }
+        for (int e = 0; e < 4; e++) { dzx[e] = vezi[e] - vez[e]; dyx[e] = vey[e] - veyi[e]; }
+        y4_h_xpml4(P, T.xb, T.py, pz, mk, dzx, dyx, store, hy, hz);
     }
     if (T.qyh_lo | T.qyh_hi) {
         float dzy[4], dxy[4];
@@ -386,8 +442,8 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
             if (!q) continue;
             const int n = P.npml[1][s];
             const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
-            y4_psi_row(P.psi_h[0][1][s], P.psi_h2[0][1][s], store, mk, P.bh[1][s][q - 1], P.ch[1][s][q - 1], P.del[1], o, dzy, DB, hx);
-            y4_psi_row(P.psi_h[2][1][s], P.psi_h2[2][1][s], store, mk, P.bh[1][s][q - 1], P.ch[1][s][q - 1], P.del[1], o, dxy, DB, hz);
+            y4_psi_row2(P.psi_h[0][1][s], P.psi_h2[0][1][s], mk, dzy, DB, hx, P.psi_h[2][1][s], P.psi_h2[2][1][s], mk, dxy,
+                        DB, hz, store, P.bh[1][s][q - 1], P.ch[1][s][q - 1], P.del[1], o);
         }
     }
     const int k = pz + 1;
@@ -400,8 +456,8 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
             const int q = s ? qz_hi : qz_lo;
             if (!q) continue;
             const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
-            y4_psi_row(P.psi_h[0][2][s], P.psi_h2[0][2][s], store, mk, P.bh[2][s][q - 1], P.ch[2][s][q - 1], P.del[2], o, dyz, DB, hx);
-            y4_psi_row(P.psi_h[1][2][s], P.psi_h2[1][2][s], store, mk, P.bh[2][s][q - 1], P.ch[2][s][q - 1], P.del[2], o, dxz, DB, hy);
+            y4_psi_row2(P.psi_h[0][2][s], P.psi_h2[0][2][s], mk, dyz, DB, hx, P.psi_h[1][2][s], P.psi_h2[1][2][s], mk, dxz,
+                        DB, hy, store, P.bh[2][s][q - 1], P.ch[2][s][q - 1], P.del[2], o);
         }
     }
     if (mk != 0xFu) {
@@ -618,7 +674,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
                         const float gax = gab[m * 6 + 0], gay = gab[m * 6 + 1], gaz = gab[m * 6 + 2];
                         const float gbx = gab[m * 6 + 3], gby = gab[m * 6 + 4], gbz = gab[m * 6 + 5];
                         float ex_n[4], ey_n[4], ez_n[4];
-    #pragma unroll
+#pragma unroll
                         for (int e = 0; e < 4; e++) {
                             ex_n[e] = gax * vex[e] + gbx * ((hz[e] - hzj[e]) * dey + (hyp[e] - hy[e]) * dez);
                             ey_n[e] = gay * vey[e] + gby * ((him_z[e] - hz[e]) * dex[e] + (hx[e] - hxp[e]) * dez);
@@ -633,38 +689,36 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
                         }
                         // CPML terms in the reference's order: Ex (y, z), Ey (x, z), Ez (x, y)
                         if (T.e_xpml) {
-    #pragma unroll
-                            for (int e = 0; e < 4; e++) {
-                                const float2 t = y4_e_xpml(P, T.xb + e, T.py, pz, him_z[e] - hz[e], hy[e] - him_y[e], gby, gbz,
-                                                           my >> e & 1u, mz >> e & 1u, ey_n[e], ez_n[e]);
-                                ey_n[e] = t.x; ez_n[e] = t.y;
-                            }
+                            float dzx[4], dyx[4];
+#pragma unroll
+                            for (int e = 0; e < 4; e++) { dzx[e] = him_z[e] - hz[e]; dyx[e] = hy[e] - him_y[e]; }
+                            y4_e_xpml4(P, T.xb, T.py, pz, my, mz, dzx, dyx, gby, gbz, ey_n, ez_n);
                         }
                         if (T.qye_lo | T.qye_hi) {
                             float dzy[4], dxy[4];
-    #pragma unroll
+#pragma unroll
                             for (int e = 0; e < 4; e++) { dzy[e] = hz[e] - hzj[e]; dxy[e] = hxj[e] - hx[e]; }
                             for (int s = 0; s < 2; s++) {
                                 const int q = s ? T.qye_hi : T.qye_lo;
                                 if (!q) continue;
                                 const int n = P.npml[1][s];
                                 const long long o = ((long long)pz * n + (q - 1)) * P.PX + T.xb;
-                                y4_psi_row(P.psi_e[0][1][s], P.psi_e[0][1][s], true, mx, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dzy, gbx, ex_n);
-                                y4_psi_row(P.psi_e[2][1][s], P.psi_e[2][1][s], true, mz, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o, dxy, gbz, ez_n);
+                                y4_psi_row2(P.psi_e[0][1][s], P.psi_e[0][1][s], mx, dzy, gbx, ex_n, P.psi_e[2][1][s], P.psi_e[2][1][s], mz,
+                                            dxy, gbz, ez_n, true, P.be[1][s][q - 1], P.ce[1][s][q - 1], P.del[1], o);
                             }
                         }
                         const int qzl = (kk >= 2 && kk <= P.npml[2][0]) ? kk : 0;
                         const int qzh = (kk >= P.Z + 1 - P.npml[2][1] && kk <= P.Z - 1) ? P.Z + 1 - kk : 0;
                         if (qzl | qzh) {
                             float dyz[4], dxz[4];
-    #pragma unroll
+#pragma unroll
                             for (int e = 0; e < 4; e++) { dyz[e] = hyp[e] - hy[e]; dxz[e] = hx[e] - hxp[e]; }
                             for (int s = 0; s < 2; s++) {
                                 const int q = s ? qzh : qzl;
                                 if (!q) continue;
                                 const long long o = ((long long)(q - 1) * P.SY + T.py) * P.PX + T.xb;
-                                y4_psi_row(P.psi_e[0][2][s], P.psi_e[0][2][s], true, mx, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dyz, gbx, ex_n);
-                                y4_psi_row(P.psi_e[1][2][s], P.psi_e[1][2][s], true, my, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o, dxz, gby, ey_n);
+                                y4_psi_row2(P.psi_e[0][2][s], P.psi_e[0][2][s], mx, dyz, gbx, ex_n, P.psi_e[1][2][s], P.psi_e[1][2][s], my,
+                                            dxz, gby, ey_n, true, P.be[2][s][q - 1], P.ce[2][s][q - 1], P.del[2], o);
                             }
                         }
                         const long long c = (long long)pz * P.plane + T.rowoff;
@@ -673,7 +727,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
                         if (mz) y4_store4(P.E2[2], c, mz, ez_n);
                     } else {
                         const int py = T.py;
-    #pragma unroll
+#pragma unroll
                         for (int e = 0; e < 4; e++) {
                             const int px = T.xb + e, i = px + 1;
                             if (px >= P.SX) continue;
