@@ -399,7 +399,7 @@ __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw,
     } else bad++;
 }
 
-__global__ void __launch_bounds__(256, 2) k_ff_bin_batch(const __grid_constant__ AemParams P,
+__global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__ AemParams P,
                                                          const __grid_constant__ FarFieldDev F, int n0, int nt) {
     extern __shared__ float hist[];  // [group][4][hspan]: U1, U2, W1, W2
     __shared__ float ksh[64][3];

@@ -480,7 +480,9 @@ void Solver::setup_farfield() {
     }
     // time batching on the FP32 path when the histograms fit in shared memory
     F.hspan = (int)std::ceil(span) + FF_TB + 8;
-    const size_t smem_max = 96 * 1024;
+    // three CTAs per SM (80 registers, at most 72 KB of histograms each):
+    // the binning is latency-bound on its shared-memory adds
+    const size_t smem_max = 72 * 1024;
     F.group = (int)std::min<size_t>(64, smem_max / ((size_t)4 * F.hspan * sizeof(float)));
     // (AEM_FF_PER_STEP=1 keeps the per-step binning kernel, for A/B checks)
     F.tb = (!d.kmax && F.group >= 1 && !getenv_flag("AEM_FF_PER_STEP")) ? FF_TB : 1;
