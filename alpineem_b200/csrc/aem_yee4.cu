@@ -69,7 +69,8 @@ constexpr int Y4_OFF_HN = Y4_OFF_I + Y4_IS * Y4_IC;
 constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+7
 constexpr int Y4_OFF_DZ = Y4_OFF_HN + Y4_HN_F * 4;
 constexpr int Y4_OFF_DX = Y4_OFF_DZ + 2 * Y4_ZC * 4;
-constexpr int Y4_OFF_GAB = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
+constexpr int Y4_OFF_XH = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
+constexpr int Y4_OFF_GAB = Y4_OFF_XH + 2 * Y4_TY * 2 * 4;
 constexpr int Y4_OFF_BAR = Y4_OFF_GAB + AEM_MAX_MATERIALS * 6 * 4;
 constexpr int Y4_SMEM = Y4_OFF_BAR + Y4_NB * 8;
 constexpr unsigned Y4_TX_E = Y4_ER * Y4_EW * 4, Y4_TX_H = Y4_HR * Y4_HW * 4, Y4_TX_I = Y4_IR * Y4_IW;
@@ -478,6 +479,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
     float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);    // [2][9][128]: hx, hz of H_new(k)
     float* dzs = reinterpret_cast<float*>(smem + Y4_OFF_DZ);   // den_h z, den_e z of the chunk's planes
     float* dxs = reinterpret_cast<float*>(smem + Y4_OFF_DX);   // den_h x, den_e x of the tile's columns
+    float* xh = reinterpret_cast<float*>(smem + Y4_OFF_XH);    // [plane & 1][row 1..8][Hy, Hz] of the -x halo cell
     float* gab = reinterpret_cast<float*>(smem + Y4_OFF_GAB);  // [mat][6]: ga xyz, gb xyz
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Y4_OFF_BAR);
     const int lane = threadIdx.x, w = threadIdx.y;
@@ -576,6 +578,24 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
     const bool tile_in = x0 >= 1 && x0 + Y4_TX - 1 <= P.SX - 2 && x0 > P.npml[0][0] &&
                          x0 + Y4_TX < P.X + 1 - P.npml[0][1] && y0 >= 1 && y0 + Y4_TY - 1 <= P.SY - 2 &&
                          y0 > P.npml[1][0] && y0 + Y4_TY < P.Y + 1 - P.npml[1][1];
+    // H_new(k) (Hy, Hz) of the -x halo cells of rows y0..y0+7, one per lane
+    // 0..7 of warp 8, into xh[k & 1]; warp 8 has no E update, so this runs
+    // while warps 0..7 update E of the plane before
+    auto xhalo_rows = [&](int k) {
+        if (lane >= Y4_TY) return;
+        const int py = y0 + lane;
+        float hyv = 0.0f, hzv = 0.0f;
+        if (py < P.SY) {
+            const int pz = zw(k), kz = pz + 1, jr = py + 1;
+            const bool cpml_yz = jr <= P.npml[1][0] - 1 || jr >= P.Y + 1 - P.npml[1][1] || kz <= P.npml[2][0] - 1 ||
+                                 kz >= P.Z + 1 - P.npml[2][1];
+            const float2 hh = y4_h_xhalo(P, Ew(k), Ew(k + 1), Hw(k), lane + 1, x0, py, pz, hzm, cpml_yz, dxs[2 * Y4_TX],
+                                         P.den_h[1][py], dzs[k - z0]);
+            hyv = hh.x; hzv = hh.y;
+        }
+        xh[((k & 1) * Y4_TY + lane) * 2 + 0] = hyv;
+        xh[((k & 1) * Y4_TY + lane) * 2 + 1] = hzv;
+    };
 
     bool ok = y4_bar_wait(&bar[0], 0);
     if (!__syncthreads_and(ok)) {
@@ -589,6 +609,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
         const int pzb = zw(z0 - 1);
         y4_h_group<false>(P, T, Ew(z0 - 1), Ew(z0), Hw(z0 - 1), pzb, hzm, P.den_h[2][pzb], dxs, dhy, false, hxp, hyp, hz_unused);
     }
+    if (w == Y4_TY) xhalo_rows(z0);
 
     for (int k = z0; k < z1; k++) {
         const int pz = zw(k);
@@ -621,21 +642,23 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
                 y4_h_group<IN>(P, T, E0, Ew(k + 1), Hw(k), pz, hzm, dhz, dxs, dhy, T.own, hx, hy, hz);
             else
                 for (int e = 0; e < 4; e++) hx[e] = hy[e] = hz[e] = 0.0f;
-            float hy_xh = 0.0f, hz_xh = 0.0f;
-            if (lane == 0 && T.own) {
-                const int kz = pz + 1;
-                const bool cpml_yz = !IN && ((T.qyh_lo | T.qyh_hi) || kz <= P.npml[2][0] - 1 || kz >= P.Z + 1 - P.npml[2][1]);
-                const float2 hh = y4_h_xhalo(P, E0, Ew(k + 1), Hw(k), T.r, x0, T.py, pz, hzm, cpml_yz, dxs[2 * Y4_TX], dhy, dhz);
-                hy_xh = hh.x; hz_xh = hh.y;
-            }
             *reinterpret_cast<float4*>(Hn + (0 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
             *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
             __syncthreads();
 
-            // ---- E_new(k) of the own rows
+            // ---- E_new(k) of the own rows; warp 8 meanwhile computes the -x
+            // halo cells of plane k+1
+            if (w == Y4_TY && k + 1 < z1) {
+                // stage k+1 (E(k+2), H(k+1)) may not have landed yet
+                ok = y4_bar_wait(&bar[(k + 1 - z0) % Y4_NB], ((k + 1 - z0) / Y4_NB) & 1) && ok;
+                if (ok) xhalo_rows(k + 1);
+            }
             if (w < Y4_TY) {
                 float hz_im0 = __shfl_up_sync(FULL, hz[3], 1), hy_im0 = __shfl_up_sync(FULL, hy[3], 1);
-                if (lane == 0) { hz_im0 = hz_xh; hy_im0 = hy_xh; }
+                if (lane == 0) {
+                    hy_im0 = xh[((k & 1) * Y4_TY + w) * 2 + 0];
+                    hz_im0 = xh[((k & 1) * Y4_TY + w) * 2 + 1];
+                }
                 if (T.own) {
                     const int r = T.r;
                     const float4 hxj4 = lds4(Hn + (0 * Y4_HR + r - 1) * Y4_TX + 4 * lane);
