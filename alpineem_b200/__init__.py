@@ -48,6 +48,8 @@ def load_library():
     lib.aem_version.restype = ctypes.c_int
     lib.aem_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(h)]
     lib.aem_run.argtypes = [h, ctypes.c_int]
+    lib.aem_run_graph.argtypes = [h, ctypes.c_int, ctypes.c_int]
+    lib.aem_run_batch.argtypes = [ctypes.POINTER(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.aem_steps.argtypes = [h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.aem_synchronize.argtypes = [h]
     lib.aem_write_outputs.argtypes = [h]
@@ -169,6 +171,11 @@ class Simulation:
     def run(self, nsteps):
         self._check(self._lib.aem_run(self._h, int(nsteps)))
 
+    def run_graph(self, nsteps, steps_per_graph=64):
+        """run() replaying one captured CUDA graph of `steps_per_graph`
+        steps for every whole chunk (same results as run())."""
+        self._check(self._lib.aem_run_graph(self._h, int(nsteps), int(steps_per_graph)))
+
     def synchronize(self):
         self._check(self._lib.aem_synchronize(self._h))
 
@@ -271,6 +278,22 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+def run_batch(sims, nsteps, steps_per_graph=64):
+    """Advance independent runs together: each Simulation (same device, its
+    own stream) replays its CUDA graph of `steps_per_graph` steps, the runs
+    round-robin, so that small grids overlap on the GPU.  Each run's results
+    equal Simulation.run()'s."""
+    sims = list(sims)
+    if not sims:
+        return
+    lib = load_library()
+    arr = (ctypes.c_void_p * len(sims))(*[s._h for s in sims])
+    rc = lib.aem_run_batch(arr, len(sims), int(nsteps), int(steps_per_graph))
+    if rc != 0:
+        msg = lib.aem_last_error(None)
+        raise RuntimeError("aem_run_batch failed (%d): %s" % (rc, msg.decode() if msg else ""))
 
 
 def run_deck(inputs_path, kmax=False, outdir=None):

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <vector>
 #include <stdexcept>
 #include <string>
 
@@ -120,6 +121,27 @@ int aem_run(aem_handle* h, int nsteps) {
     if (!h || nsteps < 0) return fail(h, AEM_ERR_ARG, "bad argument");
     return guarded(h, [&]() {
         h->s->run(nsteps);
+        return AEM_OK;
+    });
+}
+
+int aem_run_graph(aem_handle* h, int nsteps, int steps_per_graph) {
+    if (!h || nsteps < 0 || steps_per_graph < 1) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->run_graph(nsteps, steps_per_graph);
+        return AEM_OK;
+    });
+}
+
+int aem_run_batch(aem_handle* const* hs, int count, int nsteps, int steps_per_graph) {
+    if (!hs || count < 1 || nsteps < 0 || steps_per_graph < 1) return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    std::vector<aem::Solver*> v(count);
+    for (int i = 0; i < count; i++) {
+        if (!hs[i]) return fail(nullptr, AEM_ERR_ARG, "bad argument");
+        v[i] = hs[i]->s.get();
+    }
+    return guarded(nullptr, [&]() {
+        aem::Solver::run_batch(v.data(), count, nsteps, steps_per_graph);
         return AEM_OK;
     });
 }

@@ -44,6 +44,7 @@ __device__ inline float feed(const PortDev& p, int c, int a, int b) {
 // ports on the H half-step, ref :4800-5118
 template <typename T>
 __global__ void k_ports_h(const __grid_constant__ AemParams P, const __grid_constant__ PortSet S, int counter) {
+    counter = step_of(P, counter);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int n = 0; n < S.n; n++) {
@@ -132,6 +133,7 @@ __global__ void k_ports_h(const __grid_constant__ AemParams P, const __grid_cons
 // ports on the E half-step, ref :6123-6283, plus the voltage tap :8241
 template <typename T>
 __global__ void k_ports_e(const __grid_constant__ AemParams P, const __grid_constant__ PortSet S, int counter) {
+    counter = step_of(P, counter);
     const int tid = threadIdx.x;
     for (int n = 0; n < S.n; n++) {  // 1-D line voltages, ref :6125-6142
         const PortDev& p = S.p[n];
@@ -251,6 +253,7 @@ __device__ inline void atomic_add<cf>(cf* p, cf v) { atomicAdd(&p->x, v.x); atom
 // image position and sign factors)
 template <typename T>
 __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_constant__ FarFieldDev F, int counter) {
+    counter = step_of(P, counter);
     const long long cells = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]);
     const long long tot = cells * F.nang;
     T* UW = reinterpret_cast<T*>(F.UW);
@@ -401,6 +404,7 @@ __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw,
 
 __global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__ AemParams P,
                                                          const __grid_constant__ FarFieldDev F, int n0, int nt) {
+    if (P.dstep) n0 = *P.dstep - nt + 1;  // graph replay: the batch ends at the current step
     extern __shared__ float hist[];  // [group][4][hspan]: U1, U2, W1, W2
     __shared__ float ksh[64][3];
     __shared__ int bsh[64], vash[64];
@@ -493,6 +497,7 @@ __global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__
 template <typename T>
 __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constant__ TapDev D,
                        const __grid_constant__ FarFieldDev F, int counter, int steps) {
+    counter = step_of(P, counter);
     __shared__ T red[4][1024];
     const int tid = threadIdx.x;
     if (D.plane_sum) {
@@ -558,6 +563,7 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
 // 2-D video slice, ref :6833-6958 (cell-centred E, H halves at both steps)
 template <typename T>
 __global__ void k_video(const __grid_constant__ AemParams P, const __grid_constant__ TapDev D, int counter, int steps) {
+    counter = step_of(P, counter);
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= D.v1 * D.v2) return;
     const int va = q % D.v1 + 1, vb = q / D.v1 + 1;
@@ -579,6 +585,13 @@ __global__ void k_video(const __grid_constant__ AemParams P, const __grid_consta
 }
 
 // ---------------------------------------------------------------------------
+// graph replay: the step counter advances once at the end of every step
+__global__ void k_step_advance(int* d) { *d += 1; }
+int launch_step_advance(int* d, cudaStream_t s) {
+    k_step_advance<<<1, 1, 0, s>>>(d);
+    return 1;
+}
+
 int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s) {
     if (!ps.n) return 0;
     if (P.kmax) k_ports_h<cf><<<1, 512, 0, s>>>(P, ps, counter);

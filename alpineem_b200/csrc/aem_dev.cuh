@@ -68,6 +68,10 @@ __device__ __forceinline__ float cpml_div(float num, float dl) {
 }
 __device__ __forceinline__ cf cpml_div(cf num, float dl) { return {cpml_div(num.x, dl), cpml_div(num.y, dl)}; }
 
+// the step number of this launch: the device counter during graph replay,
+// else the launch argument
+__device__ __forceinline__ int step_of(const AemParams& P, int counter) { return P.dstep ? *P.dstep : counter; }
+
 __device__ inline long long lin(const AemParams& P, int px, int py, int pz) {
     return ((long long)pz * P.SY + py) * P.PX + px;
 }

@@ -52,6 +52,7 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemParams P, int counter) {
+    counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * 8 + threadIdx.y;
     // H is updated on reference indices 1..N-1 of every axis (all positions
@@ -312,6 +313,7 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemParams P, int counter) {
+    counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * 8 + threadIdx.y;
     if (px >= P.SX || py >= P.SY) return;

@@ -128,6 +128,7 @@ void Solver::setup_fused() {
 
 void Solver::release() {
     if (stream_) cudaStreamSynchronize(stream_);
+    release_graph();
     for (void* p : bufs_) cudaFree(p);
     bufs_.clear();
     for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
@@ -697,6 +698,102 @@ void Solver::run(int n) {
     // partial batches wait for more steps (or for flush())
     if (done_ == m_.d.steps) flush_farfield(done_);
     AEM_CUDA(cudaGetLastError());
+}
+
+void Solver::release_graph() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    graph_g_ = 0;
+}
+
+bool Solver::graph_ready(int g) const {
+    if (g < 1 || done_ == 0 || done_ + g > m_.d.steps) return false;  // the first step runs eagerly
+    if (fused_ && (g & 1)) return false;                                // an even number of buffer swaps
+    if (FF_.tb > 1 && (g % FF_.tb != 0 || ff_n0_ != done_ + 1)) return false;  // whole far-field batches
+    return true;
+}
+
+// Record g steps (each followed by the counter advance) on the solver's
+// stream without running them; the host-side state the recording moved on
+// (far-field batch start, launch count) is put back, replays move it.
+void Solver::capture_graph(int g) {
+    release_graph();
+    if (!dstep_) dstep_ = (int*)alloc(sizeof(int));
+    const int n0 = ff_n0_;
+    const long long l0 = launches_;
+    const bool prof = prof_on_;
+    prof_on_ = false;
+    P_.dstep = dstep_;
+    cudaGraph_t graph = nullptr;
+    AEM_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int q = 1; q <= g; q++) {
+            step(done_ + q);
+            launches_ += launch_step_advance(dstep_, stream_);
+        }
+    } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        P_.dstep = nullptr;
+        ff_n0_ = n0;
+        launches_ = l0;
+        prof_on_ = prof;
+        throw;
+    }
+    P_.dstep = nullptr;
+    ff_n0_ = n0;
+    prof_on_ = prof;
+    graph_launches_ = launches_ - l0;
+    launches_ = l0;
+    AEM_CUDA(cudaStreamEndCapture(stream_, &graph));
+    cudaError_t e = cudaGraphInstantiate(&graph_, graph, 0);
+    cudaGraphDestroy(graph);
+    AEM_CUDA(e);
+    graph_g_ = g;
+}
+
+void Solver::run_graph(int n, int g) {
+    Solver* self = this;
+    run_batch(&self, 1, n, g);
+}
+
+void Solver::run_batch(Solver* const* s, int count, int n, int g) {
+    std::vector<int> left(count);
+    for (int i = 0; i < count; i++) {
+        Solver& v = *s[i];
+        left[i] = std::max(0, std::min(n, v.m_.d.steps - v.done_));
+        // eager steps until a chunk can start (at most one far-field batch)
+        while (left[i] > 0 && !v.graph_ready(g) && (v.done_ == 0 || left[i] < g || v.FF_.tb > 1 && v.ff_n0_ != v.done_ + 1)) {
+            v.run(1);
+            left[i]--;
+        }
+        if (left[i] >= g && v.graph_ready(g)) {
+            if (!v.graph_ || v.graph_g_ != g) v.capture_graph(g);
+            const int next = v.done_ + 1;
+            AEM_CUDA(cudaMemcpyAsync(v.dstep_, &next, sizeof next, cudaMemcpyHostToDevice, v.stream_));
+            v.h2d_bytes_ += sizeof next;
+        }
+    }
+    // whole chunks, round-robin over the solvers
+    for (bool any = true; any;) {
+        any = false;
+        for (int i = 0; i < count; i++) {
+            Solver& v = *s[i];
+            if (!v.graph_ || left[i] < g || v.done_ + g > v.m_.d.steps) continue;
+            AEM_CUDA(cudaGraphLaunch(v.graph_, v.stream_));
+            v.done_ += g;
+            left[i] -= g;
+            v.launches_ += v.graph_launches_;
+            if (v.FF_.tb > 1) v.ff_n0_ = v.done_ + 1;
+            any = true;
+        }
+    }
+    // the rest eagerly (run() also bins the last far-field batch)
+    for (int i = 0; i < count; i++) {
+        Solver& v = *s[i];
+        if (left[i] > 0 || v.done_ == v.m_.d.steps) v.run(left[i]);
+    }
 }
 
 }  // namespace aem

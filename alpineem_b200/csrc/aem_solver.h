@@ -32,6 +32,17 @@ class Solver {
 
     // advance `n` time steps (bounded by the deck's step count)
     void run(int n);
+    // Advance `n` steps, replaying a captured CUDA graph of `g` steps for
+    // every whole chunk: the kernels read the step number from a device
+    // counter, so one graph serves every chunk.  Steps before the first chunk
+    // (the first step of a run; far-field batch alignment) and after the last
+    // run eagerly.  Graph chunks need g even on the fused path (the field
+    // buffers swap each step) and g a multiple of the far-field batch.
+    void run_graph(int n, int g);
+    // the launch part of run_graph for a batch of solvers on their own
+    // streams: every solver gets to the same point, then the chunks of all
+    // solvers are launched round-robin so that their graphs overlap
+    static void run_batch(Solver* const* s, int count, int n, int g);
     // post-loop processing and the reference output files (.dat, video)
     void finalize_and_write();
     // host copy of a final field component in the reference layout
@@ -84,6 +95,9 @@ class Solver {
     void setup_fused();
     void step(int counter);
     void flush_farfield(int last);
+    bool graph_ready(int g) const;  // can a g-step graph chunk start at the next step?
+    void capture_graph(int g);
+    void release_graph();
     template <typename Fn>
     void phase(int ph, Fn&& fn);
     cudaEvent_t prof_event();
@@ -116,6 +130,11 @@ class Solver {
     size_t prof_used_ = 0;
     std::vector<ProfMark> prof_marks_;
     cudaStream_t stream_ = nullptr;
+    // graph replay
+    int* dstep_ = nullptr;          // device step counter
+    cudaGraphExec_t graph_ = nullptr;
+    int graph_g_ = 0;               // steps per graph
+    long long graph_launches_ = 0;  // kernels per replay
 };
 
 }  // namespace aem

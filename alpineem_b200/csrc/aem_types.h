@@ -126,4 +126,7 @@ struct AemParams {
     void* psi_h2[3][3][2];
     // device counter of fused-step CTAs that gave up a bounded wait (0 = ok)
     int* err;
+    // graph replay: the step number (1-based) lives in device memory and the
+    // kernels read it instead of their `counter` argument (null: eager steps)
+    const int* dstep;
 };

@@ -73,6 +73,22 @@ int aem_check_deck(const char* deck_text, const char* ext_text, int mode, int si
  * one `counter` per step), never past the deck's step count. */
 int aem_run(aem_handle* h, int nsteps);
 
+/* aem_run with CUDA-graph replay: `steps_per_graph` steps are captured once
+ * and replayed for every whole chunk (the kernels read the step number from
+ * device memory).  Results equal aem_run's.  Steps before the first chunk
+ * (the run's first step, far-field batch alignment) and the remainder run as
+ * aem_run does.  The fused path needs an even chunk, far-field batching a
+ * multiple of its 32-step batch.  No reference counterpart: the reference
+ * launches every loop body from the host (fdtd_solver.f90:4440-8299). */
+int aem_run_graph(aem_handle* h, int nsteps, int steps_per_graph);
+
+/* Advance `count` independent runs (distinct handles on the same device,
+ * each on its own stream) by `nsteps` each, replaying their graphs
+ * round-robin so that small grids overlap on the GPU.  Each run's results
+ * equal aem_run's.  This is the batched-instance driver that replaces the
+ * reference's process-level fan-out (utility_scripts/parallel_kmax.py). */
+int aem_run_batch(aem_handle* const* handles, int count, int nsteps, int steps_per_graph);
+
 /* Raw per-step samples of the steps run so far, before the normalisation
  * that aem_write_outputs applies: kind 5 = voltage of port `index`
  * (Voltage_out, fdtd_solver.f90:8241-8243), kind 1 / 2 = reflected /
