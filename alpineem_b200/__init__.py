@@ -71,6 +71,7 @@ def load_library():
     lib.aem_profile_read.argtypes = [h, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     lib.aem_launch_count.argtypes = [h, ctypes.POINTER(ctypes.c_longlong)]
     lib.aem_workload.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
+    lib.aem_far_field_size.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
     lib.aem_flush.argtypes = [h]
     lib.aem_dft.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
                             ctypes.c_void_p, ctypes.c_void_p]
@@ -261,6 +262,14 @@ class Simulation:
         c, b = ctypes.c_longlong(), ctypes.c_double()
         self._check(self._lib.aem_workload(self._h, ctypes.byref(c), ctypes.byref(b)))
         return c.value, b.value
+
+    @property
+    def far_field_size(self):
+        """(Huygens-surface cells, far-field angles): each step bins their
+        product of contributions."""
+        c, a = ctypes.c_longlong(), ctypes.c_int()
+        self._check(self._lib.aem_far_field_size(self._h, ctypes.byref(c), ctypes.byref(a)))
+        return c.value, a.value
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

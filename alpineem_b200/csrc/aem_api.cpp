@@ -268,6 +268,16 @@ int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step) {
     return AEM_OK;
 }
 
+int aem_far_field_size(aem_handle* h, long long* face_cells, int* angles) {
+    if (!h) return AEM_ERR_ARG;
+    long long fc = 0;
+    int na = 0;
+    h->s->far_field_size(&fc, &na);
+    if (face_cells) *face_cells = fc;
+    if (angles) *angles = na;
+    return AEM_OK;
+}
+
 int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream) {
     if (!x || !freqs || !out || n < 1 || nf < 1 || !(dt > 0.0)) return fail(nullptr, AEM_ERR_ARG, "bad argument");
     cudaStream_t s = (cudaStream_t)stream;

@@ -71,6 +71,11 @@ class Solver {
     void read_probe(int kind, int index, int first, int n, double* re, double* im);
     // bytes the fused Yee/CPML update must move per step (algorithmic)
     double algorithmic_bytes_per_step() const;
+    // Huygens-surface cells (both planes of each axis) and far-field angles
+    void far_field_size(long long* face_cells, int* angles) const {
+        *face_cells = 2 * (FF_.face_n[0] + FF_.face_n[1] + FF_.face_n[2]);
+        *angles = FF_.nang;
+    }
     long long cell_count() const;
 
     // time series gathered on the host by finalize

@@ -64,3 +64,47 @@ def dipole_ellipsoids(n=1024, steps=4000, n_ell=64, seed=2, pml_cells=16, dl="2E
              ports=[("basic", "z", 50, (c, c, c), (1, 1, 1))])
     ext = "pml_cells %d\ngeometry_bin no\n" % pml_cells
     return d, ext, bulk
+
+
+def kmax_batch(n_inst=64, steps=6000, seed=3, dl="1E-3", f="10E9", nxy=64, depth=10, patch=16):
+    """Batched constant-k unit cells (the fan-out that
+    utility_scripts/parallel_kmax.py runs as separate processes): n_inst decks
+    of nxy x nxy x Z cells, periodic in x and y with CPML on z, Z drawn from
+    {128, 192, 256, 384, 512} (numpy default_rng(seed)).  Instance q has
+    incidence theta = 2.5 * (q // 2) degrees in the x-z plane, TE for even q
+    and TM for odd q, k1 = 2 pi f sin(theta) / c, k2 = 0.  Every cell holds a
+    `depth`-cell eps_r = 3, sigma = 0.002 slab under a 0-ohm (PEC) sheet
+    drawn from a patch x patch binary pattern (fill 0.5, the same seed), runs
+    of set pixels merged into sheet rectangles.  Returns a list of deck
+    dicts for alpineem_b200.deck.deck_text (kmax)."""
+    rng = np.random.default_rng(seed)
+    zs = rng.choice([128, 192, 256, 384, 512], size=n_inst)
+    bits = rng.random((patch, patch)) < 0.5
+    cell = nxy // patch
+    sheets = []
+    for r in range(patch):
+        c = 0
+        while c < patch:
+            if not bits[r, c]:
+                c += 1
+                continue
+            c1 = c
+            while c1 < patch and bits[r, c1]:
+                c1 += 1
+            sheets.append((c * cell + 1, r * cell + 1, (c1 - c) * cell, cell))
+            c = c1
+    fval = float(f)
+    decks_ = []
+    for q in range(n_inst):
+        Z = int(zs[q])
+        theta = np.deg2rad(2.5 * (q // 2))
+        k1 = 2.0 * np.pi * fval * np.sin(theta) / 299792458.0
+        z0 = Z // 2 - depth // 2
+        d = dict(kmax=True, n=(nxy, nxy, Z), dl=(dl, dl, dl), steps=steps, f=f, pulse=2, bc=(1, 1, 1, 1, 0, 0),
+                 excitation=("plane wave", 1, 0, "TE" if q % 2 == 0 else "TM", "+"), k=("%.6f" % k1, "0.0"),
+                 name="data.dat",
+                 mats=[("simple", 2, (3, 3, 3), (0.002, 0.002, 0.002)), ("sheet", 3, 0)],
+                 objects=[("block", 2, (1, 1, z0), (nxy, nxy, depth))],
+                 sheets=[("z", 3, z0 + depth, (a, b), (sa, sb)) for a, b, sa, sb in sheets])
+        decks_.append(d)
+    return decks_

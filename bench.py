@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--cpu-steps", type=int, default=8, help="timed steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched kmax-instance measurement")
+    ap.add_argument("--batch-steps", type=int, default=192, help="timed steps of every batched instance")
+    ap.add_argument("--batch-graph", type=int, default=32, help="steps per captured CUDA graph")
     return ap.parse_args()
 
 
@@ -191,6 +194,55 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
+    """The batched constant-k sweep (64 unit cells, workloads.kmax_batch):
+    wall time of the instances run one after another with plain launches,
+    against the same instances advanced together by aem_run_batch (one
+    stream per instance, one CUDA graph of g steps per instance).  Ranks
+    take every world-th instance.  Setup, a 4-step warm-up of each run and
+    the graph capture (one untimed chunk) are outside both timings."""
+    import alpineem_b200 as ab
+    from alpineem_b200 import workloads
+    from alpineem_b200.deck import deck_text
+
+    warm = 4
+    decks = workloads.kmax_batch(steps=warm + 2 * g + steps)[rank::world]
+    tmp = tempfile.mkdtemp(prefix="aem_batch_")
+    seq = 0.0
+    cells = 0
+    for d in decks:
+        sim = ab.Simulation(deck_text=deck_text(d), kmax=True, outdir=tmp)
+        cells += sim.workload[0]
+        sim.run(warm + g)
+        sim.synchronize()
+        t0 = time.perf_counter()
+        sim.run(steps)
+        sim.synchronize()
+        seq += time.perf_counter() - t0
+        sim.close()
+    sims = [ab.Simulation(deck_text=deck_text(d), kmax=True, outdir=tmp) for d in decks]
+    try:
+        for s in sims:
+            s.run(warm)
+        ab.run_batch(sims, g, g)  # captures every instance's graph
+        for s in sims:
+            s.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ab.run_batch(sims, steps, g)
+        for s in sims:
+            s.synchronize()
+        bat = time.perf_counter() - t0
+    finally:
+        for s in sims:
+            s.close()
+    seq, bat = max_over_ranks(seq), max_over_ranks(bat)
+    return {"workload": "kmax_batch", "instances": 64, "grid": "64 x 64 x Z, Z in {128..512}, complex64",
+            "steps_timed": steps, "steps_per_graph": g, "sequential_s": round(seq, 4), "batched_s": round(bat, 4),
+            "speedup": round(seq / bat, 2),
+            "batched_mcell_updates_per_s": round(world * cells * steps / bat / 1e6, 1)}
+
+
 def ours(args):
     import torch
     import alpineem_b200 as ab
@@ -261,6 +313,13 @@ def ours(args):
                 "traffic": round(ratio * bytes_step) if ratio else None,
                 "algorithmic_bytes": round(bytes_step), "bytes_per_cell_update": round(bytes_step / cells, 2)}
     phases = {k: round(v[0] / K, 4) for k, v in prof.items() if v[1]}
+    ff_cells, ff_angles = sim.far_field_size
+    far_field = None
+    if prof["ff_bin"][1] and prof["ff_bin"][0] > 0:
+        contrib = ff_cells * ff_angles
+        far_field = {"metric": "binned far-field contributions/s", "face_cells": ff_cells, "angles": ff_angles,
+                     "contributions_per_step": contrib, "ms_per_step": round(prof["ff_bin"][0] / K, 4),
+                     "value": round(world * contrib / (prof["ff_bin"][0] / K / 1e3), 1)}
     sim.close()
     del sim
 
@@ -287,6 +346,10 @@ def ours(args):
                "h2d_bytes_per_step": round(h2d / K), "d2h_bytes_per_step": round(d2h / K),
                "seconds": round(wall, 3), "steps": K}
 
+    batched = None
+    if not args.no_batch:
+        batched = batched_kmax(rank, world, args.batch_steps, args.batch_graph, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, threads, ccells = oracle_sample(args.cpu_n, 1, args.cpu_steps)
@@ -304,7 +367,8 @@ def ours(args):
                            "l2": "no flush: 28 GB of resident fields and tables, far above the 126 MB L2",
                            "parallelism": "replicas" if world > 1 else "single"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": launches, "phases_ms_per_step": phases,
+                "gpu_launches": launches, "phases_ms_per_step": phases, "far_field": far_field,
+                "batched_kmax": batched,
                 "setup_s": round(t_setup, 2), "workload_gen_s": round(t_gen, 2)}
         print(json.dumps(line), flush=True)
     if dist:

@@ -137,6 +137,11 @@ int aem_transfer_bytes(aem_handle* h, long long* h2d, long long* d2h);
  * 8 CPML psi values per cell of each CPML slab. */
 int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step);
 
+/* Far-field work of one step: Huygens-surface cells (both planes of every
+ * non-periodic axis, fdtd_solver.f90:7512-7641) and far-field angles; each
+ * step bins face_cells x angles contributions (:7643-7925). */
+int aem_far_field_size(aem_handle* h, long long* face_cells, int* angles);
+
 /* Spectrum of a time series at arbitrary frequencies, on the GPU:
  *   out[2k] + i out[2k+1] = sum_{m<n} x[m] exp(-i 2 pi freqs[k] m dt).
  * x (n floats), freqs (nf doubles, Hz) and out (2*nf doubles) are device
