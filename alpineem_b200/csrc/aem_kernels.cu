@@ -50,6 +50,10 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
     return nw;
 }
 
+// z planes per CTA of the two-kernel path: a grid narrow in x and y (a
+// kmax unit cell) still spreads over every SM
+constexpr int UPD_ZCH = 16;
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
@@ -76,7 +80,10 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
     const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0;
     const int qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
 
-    for (int pz = 0; pz <= hz; pz++) {
+    // this CTA's z chunk (planes are independent: every plane reloads its
+    // neighbours)
+    const int pz_end = min(hz, ((int)blockIdx.z + 1) * UPD_ZCH - 1);
+    for (int pz = blockIdx.z * UPD_ZCH; pz <= pz_end; pz++) {
         bool wz;
         const int pzn = wrap_up(P, 2, pz, P.SZ, &wz);
         const int k = pz + 1;
@@ -228,42 +235,56 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
 
 // Material coefficients of one E edge: sheet override, index-1 vacuum
 // default, uniform-neighbourhood table or the reference's 4-cell average.
+// The Drude coefficients of the edge are not kept here (they would live in
+// local memory): drude_coef recomputes them from the ids inside the Drude box.
 struct EdgeCoef {
     float ga, gb;
-    float ja[AEM_MAX_POLES], jb[AEM_MAX_POLES];
+    int i0, i1, i2, i3;  // the four cell ids
+    bool uni;            // the four ids are equal: table values
 };
+
+// Ja, Jb of pole p of an edge, ref :2859-2895 (4-cell average of wp, gamma)
+__device__ inline void drude_coef(const AemParams& P, int c, const EdgeCoef& co, int p, float& ja, float& jb) {
+    if (co.uni) {
+        ja = P.ucoef[co.i0].ja[p][c];
+        jb = P.ucoef[co.i0].jb[p][c];
+        return;
+    }
+    const AemMaterial *m0 = P.mat + co.i0, *m1 = P.mat + co.i1, *m2 = P.mat + co.i2, *m3 = P.mat + co.i3;
+    const float w = (m0->wp[p][c] + m1->wp[p][c] + m2->wp[p][c] + m3->wp[p][c]) / 4.0f;
+    const float g = (m0->gam[p][c] + m1->gam[p][c] + m2->gam[p][c] + m3->gam[p][c]) / 4.0f;
+    ja = d_ja(g, P.dt);
+    jb = d_jb(w, g, P.dt);
+}
 
 __device__ inline void edge_coef(const AemParams& P, int c, int px, int py, int pz, int pxd, int pyd, int pzd,
                                  bool unaveraged, EdgeCoef& o) {
-    int id[4];
     if (unaveraged) {
-        id[0] = id[1] = id[2] = id[3] = 0;
+        o.i0 = o.i1 = o.i2 = o.i3 = 0;
     } else {
         // four cells around the edge, ref :2516-2527
         const uint8_t* C = P.cell;
-        id[0] = C[lin(P, px, py, pz)];
-        if (c == 0) { id[1] = C[lin(P, px, pyd, pz)]; id[2] = C[lin(P, px, py, pzd)]; id[3] = C[lin(P, px, pyd, pzd)]; }
-        else if (c == 1) { id[1] = C[lin(P, pxd, py, pz)]; id[2] = C[lin(P, px, py, pzd)]; id[3] = C[lin(P, pxd, py, pzd)]; }
-        else { id[1] = C[lin(P, pxd, py, pz)]; id[2] = C[lin(P, px, pyd, pz)]; id[3] = C[lin(P, pxd, pyd, pz)]; }
+        o.i0 = C[lin(P, px, py, pz)];
+        if (c == 0) { o.i1 = C[lin(P, px, pyd, pz)]; o.i2 = C[lin(P, px, py, pzd)]; o.i3 = C[lin(P, px, pyd, pzd)]; }
+        else if (c == 1) { o.i1 = C[lin(P, pxd, py, pz)]; o.i2 = C[lin(P, px, py, pzd)]; o.i3 = C[lin(P, pxd, py, pzd)]; }
+        else { o.i1 = C[lin(P, pxd, py, pz)]; o.i2 = C[lin(P, px, pyd, pz)]; o.i3 = C[lin(P, pxd, pyd, pz)]; }
     }
-    if (id[0] == id[1] && id[0] == id[2] && id[0] == id[3]) {
-        const AemUniformCoef& u = P.ucoef[id[0]];
+    o.uni = o.i0 == o.i1 && o.i0 == o.i2 && o.i0 == o.i3;
+    if (o.uni) {
+        const AemUniformCoef& u = P.ucoef[o.i0];
         o.ga = u.ga[c];
         o.gb = u.gb[c];
-        for (int p = 0; p < P.npoles; p++) { o.ja[p] = u.ja[p][c]; o.jb[p] = u.jb[p][c]; }
         return;
     }
-    const AemMaterial *m0 = P.mat + id[0], *m1 = P.mat + id[1], *m2 = P.mat + id[2], *m3 = P.mat + id[3];
+    const AemMaterial *m0 = P.mat + o.i0, *m1 = P.mat + o.i1, *m2 = P.mat + o.i2, *m3 = P.mat + o.i3;
     const float e = (m0->eps[c] + m1->eps[c] + m2->eps[c] + m3->eps[c]) / 4.0f;
     const float s = (m0->sig[c] + m1->sig[c] + m2->sig[c] + m3->sig[c]) / 4.0f;
     float tp = 0.0f;
     for (int p = 0; p < P.npoles; p++) {
-        const float w = (m0->wp[p][c] + m1->wp[p][c] + m2->wp[p][c] + m3->wp[p][c]) / 4.0f;
-        const float g = (m0->gam[p][c] + m1->gam[p][c] + m2->gam[p][c] + m3->gam[p][c]) / 4.0f;
-        o.ja[p] = d_ja(g, P.dt);
-        o.jb[p] = d_jb(w, g, P.dt);
+        float ja, jb;
+        drude_coef(P, c, o, p, ja, jb);
+        tp = tp + jb;
     }
-    for (int p = 0; p < P.npoles; p++) tp = tp + o.jb[p];
     o.ga = d_ga(s + tp, e, P.dt);
     o.gb = d_gb(s + tp, e, P.dt);
 }
@@ -299,10 +320,17 @@ __device__ inline T drude_update(const AemParams& P, int c, int px, int py, int 
     void* J = P.jsrc[c];
     const long long vol = (long long)nx * ny * nz, base = ((long long)lz * ny + ly) * nx + lx;
     T t = zero<T>();
-    for (int p = 0; p < P.npoles; p++) t = t + (1.0f + co.ja[p]) * ld<T>(J, p * vol + base);
+    for (int p = 0; p < P.npoles; p++) {
+        float ja, jb;
+        drude_coef(P, c, co, p, ja, jb);
+        t = t + (1.0f + ja) * ld<T>(J, p * vol + base);
+    }
     const T e = e_new - gb * t / 2.0f;
-    for (int p = 0; p < P.npoles; p++)
-        st<T>(J, p * vol + base, co.ja[p] * ld<T>(J, p * vol + base) + co.jb[p] * (e + e_old));
+    for (int p = 0; p < P.npoles; p++) {
+        float ja, jb;
+        drude_coef(P, c, co, p, ja, jb);
+        st<T>(J, p * vol + base, ja * ld<T>(J, p * vol + base) + jb * (e + e_old));
+    }
     return e;
 }
 
@@ -312,7 +340,7 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemParams P, int counter) {
+__global__ void __launch_bounds__(256, 2) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * 8 + threadIdx.y;
@@ -344,7 +372,8 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemPar
     const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
     const bool x_unavg = !P.per[0] && i == 1, y_unavg = !P.per[1] && j == 1;
 
-    for (int pz = 0; pz < P.SZ; pz++) {
+    const int pz_end = min(P.SZ, ((int)blockIdx.z + 1) * UPD_ZCH);
+    for (int pz = blockIdx.z * UPD_ZCH; pz < pz_end; pz++) {
         const bool ex_u = ex_xy && upd(2, pz, false), ey_u = ey_xy && upd(2, pz, false), ez_u = ez_xy && upd(2, pz, true);
         if (!ex_u && !ey_u && !ez_u) continue;
         bool wzd;
@@ -491,13 +520,13 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ AemPar
 
 // ---------------------------------------------------------------------------
 int launch_update_h(const AemParams& P, int counter, cudaStream_t s) {
-    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
+    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8, (P.SZ + UPD_ZCH - 1) / UPD_ZCH);
     if (P.kmax) k_update_h<cf><<<grd, blk, 0, s>>>(P, counter);
     else k_update_h<float><<<grd, blk, 0, s>>>(P, counter);
     return 1;
 }
 int launch_update_e(const AemParams& P, int counter, cudaStream_t s) {
-    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8);
+    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8, (P.SZ + UPD_ZCH - 1) / UPD_ZCH);
     if (P.kmax) k_update_e<cf><<<grd, blk, 0, s>>>(P, counter);
     else k_update_e<float><<<grd, blk, 0, s>>>(P, counter);
     return 1;
