@@ -195,6 +195,7 @@ def reference_arm(args):
 
 
 def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
+    from alpineem_b200.parallel import shard
     """The batched constant-k sweep (64 unit cells, workloads.kmax_batch):
     wall time of the instances run one after another with plain launches,
     against the same instances advanced together by aem_run_batch (one
@@ -206,7 +207,7 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
     from alpineem_b200.deck import deck_text
 
     warm = 4
-    decks = workloads.kmax_batch(steps=warm + 2 * g + steps)[rank::world]
+    decks = shard(workloads.kmax_batch(steps=warm + 2 * g + steps), rank, world)
     tmp = tempfile.mkdtemp(prefix="aem_batch_")
     seq = 0.0
     cells = 0
