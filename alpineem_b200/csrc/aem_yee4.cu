@@ -9,20 +9,20 @@
 // the assembler fuses a packed multiply into a following packed add even
 // with .rn and contraction disabled, which changes the rounding.)
 //
-// A CTA owns a 128 x 8 (x, y) column tile and marches a z chunk of 64
-// planes.  Warps 0..7 own rows y0..y0+7; lane l owns the four cells
+// A CTA owns a 128 x 15 (x, y) column tile and marches a z chunk of 64
+// planes.  Warps 0..14 own rows y0..y0+14; lane l owns the four cells
 // x0+4l .. x0+4l+3, so every shared-memory and global access of a cell
-// group is one 16-byte operation.  Warp 8 computes Hx, Hz of the -y halo
-// row (y0-1), which the E update of row y0 needs; lane 0 of warps 0..7
-// computes Hy, Hz of the -x halo cell (x0-1).
+// group is one 16-byte operation.  Warp 15 computes Hx, Hz of the -y halo
+// row (y0-1), which the E update of row y0 needs, and, while the others
+// update E, Hy, Hz of the -x halo cells (x0-1) of the next plane.
 //
 // Per plane p one thread requests by TMA (cp.async.bulk.tensor, zero fill
-// outside the grid) E_old(p) on rows y0-1..y0+8, x0-4..x0+131; H_old(p) on
-// rows y0-1..y0+7, x0-4..x0+127; the material ids of rows y0-1..y0+7,
+// outside the grid) E_old(p) on rows y0-1..y0+15, x0-4..x0+131; H_old(p) on
+// rows y0-1..y0+14, x0-4..x0+127; the material ids of rows y0-1..y0+14,
 // x0-16..x0+127.  Stage t (E(t+1), H(t), ids(t)) completes on its own
 // mbarrier; it is requested two planes ahead, while plane t-2 is computed,
 // into rings of 4 E planes, 3 H planes and 4 id planes.  One CTA per SM
-// (about 132 KB of shared memory).  Fields and H-psi are double-buffered
+// (about 217 KB of shared memory).  Fields and H-psi are double-buffered
 // (read E/H/psi_h, write E2/H2/psi_h2), so halo values recomputed here
 // never race with their owners' stores.
 //
@@ -50,10 +50,12 @@
 
 namespace aem {
 
-constexpr int Y4_TX = 128, Y4_TY = 8, Y4_ZC = 64, Y4_NT = 32 * (Y4_TY + 1);
-constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;   // E box 136 x 10, x from x0-4, y from y0-1
-constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;   // H box 132 x 9
-constexpr int Y4_IW = Y4_TX + 16, Y4_IR = Y4_TY + 1;  // id box 144 x 9 bytes, x from x0-16
+// 15 owned rows + the -y halo row: 16 warps (512 threads) of at most 128
+// registers, one CTA per SM; the warps hide each other's latency
+constexpr int Y4_TX = 128, Y4_TY = 15, Y4_ZC = 64, Y4_NT = 32 * (Y4_TY + 1);
+constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;   // E box 136 x 17, x from x0-4, y from y0-1
+constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;   // H box 132 x 16
+constexpr int Y4_IW = Y4_TX + 16, Y4_IR = Y4_TY + 1;  // id box 144 x 16 bytes, x from x0-16
 // every TMA destination starts on a 128-byte boundary
 constexpr int y4_up128(int b) { return (b + 127) / 128 * 128; }
 constexpr int Y4_EC = y4_up128(Y4_ER * Y4_EW * 4) / 4;  // floats from one E component tile to the next
@@ -66,7 +68,7 @@ constexpr int Y4_ES = Y4_LA + 2, Y4_HS = Y4_LA + 1, Y4_IS = Y4_LA + 2, Y4_NB = Y
 constexpr int Y4_OFF_H = Y4_ES * 3 * Y4_EC * 4;
 constexpr int Y4_OFF_I = Y4_OFF_H + Y4_HS * 3 * Y4_HC * 4;
 constexpr int Y4_OFF_HN = Y4_OFF_I + Y4_IS * Y4_IC;
-constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+7
+constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+14
 constexpr int Y4_OFF_DZ = Y4_OFF_HN + Y4_HN_F * 4;
 constexpr int Y4_OFF_DX = Y4_OFF_DZ + 2 * Y4_ZC * 4;
 constexpr int Y4_OFF_XH = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
@@ -367,7 +369,7 @@ __device__ __forceinline__ float2 y4_h_xhalo(const AemParams& P, const float* E0
 // per-thread constants of the z march
 struct Y4Row {
     int r, py, xb, xi, xbi;
-    bool own;        // warps 0..7 on a stored row
+    bool own;        // an owned-row warp on a stored row
     bool hrow;       // the row computes H (own rows and the -y halo row)
     unsigned hmask;  // cells of the group inside the H update range in x and y (bit e: cell xb+e)
     bool h_xpml;     // a cell of the group lies in an x CPML slab (H)
@@ -476,10 +478,10 @@ __device__ __forceinline__ void y4_h_group(const AemParams& P, const Y4Row& T, c
 
 __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemParams P, const __grid_constant__ Y4Maps M) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);    // [2][9][128]: hx, hz of H_new(k)
+    float* Hn = reinterpret_cast<float*>(smem + Y4_OFF_HN);    // [2][16][128]: hx, hz of H_new(k)
     float* dzs = reinterpret_cast<float*>(smem + Y4_OFF_DZ);   // den_h z, den_e z of the chunk's planes
     float* dxs = reinterpret_cast<float*>(smem + Y4_OFF_DX);   // den_h x, den_e x of the tile's columns
-    float* xh = reinterpret_cast<float*>(smem + Y4_OFF_XH);    // [plane & 1][row 1..8][Hy, Hz] of the -x halo cell
+    float* xh = reinterpret_cast<float*>(smem + Y4_OFF_XH);    // [plane & 1][row 1..15][Hy, Hz] of the -x halo cell
     float* gab = reinterpret_cast<float*>(smem + Y4_OFF_GAB);  // [mat][6]: ga xyz, gb xyz
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Y4_OFF_BAR);
     const int lane = threadIdx.x, w = threadIdx.y;
@@ -574,13 +576,13 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
     const float dhy = yin ? P.den_h[1][T.py] : 0.0f, dey = yin ? P.den_e[1][T.py] : 0.0f;
     // the tile (with its -x / -y halo) inside the update range and outside
     // the x and y CPML slabs of H and E (reference indices x0..x0+128,
-    // y0..y0+8)
+    // y0..y0+15)
     const bool tile_in = x0 >= 1 && x0 + Y4_TX - 1 <= P.SX - 2 && x0 > P.npml[0][0] &&
                          x0 + Y4_TX < P.X + 1 - P.npml[0][1] && y0 >= 1 && y0 + Y4_TY - 1 <= P.SY - 2 &&
                          y0 > P.npml[1][0] && y0 + Y4_TY < P.Y + 1 - P.npml[1][1];
-    // H_new(k) (Hy, Hz) of the -x halo cells of rows y0..y0+7, one per lane
-    // 0..7 of warp 8, into xh[k & 1]; warp 8 has no E update, so this runs
-    // while warps 0..7 update E of the plane before
+    // H_new(k) (Hy, Hz) of the -x halo cells of rows y0..y0+14, one per
+    // lane 0..14 of the halo warp, into xh[k & 1]; that warp has no E update,
+    // so this runs while the others update E of the plane before
     auto xhalo_rows = [&](int k) {
         if (lane >= Y4_TY) return;
         const int py = y0 + lane;
@@ -635,7 +637,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
         float hx[4], hy[4], hz[4];
         auto plane = [&](auto in_tag) {
             constexpr bool IN = decltype(in_tag)::value;
-            // ---- H_new(k): own rows, the -y halo row (warp 8), the -x halo cell (lane 0)
+            // ---- H_new(k): own rows and the -y halo row (halo warp)
             const float* E0 = Ew(k);
             const float dhz = dzs[k - z0], dez = dzs[Y4_ZC + k - z0];
             if (T.hrow)
@@ -646,7 +648,7 @@ __global__ void __launch_bounds__(Y4_NT, 1) k_yee4(const __grid_constant__ AemPa
             *reinterpret_cast<float4*>(Hn + (1 * Y4_HR + T.r) * Y4_TX + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
             __syncthreads();
 
-            // ---- E_new(k) of the own rows; warp 8 meanwhile computes the -x
+            // ---- E_new(k) of the own rows; the halo warp meanwhile computes the -x
             // halo cells of plane k+1
             if (w == Y4_TY && k + 1 < z1) {
                 // stage k+1 (E(k+2), H(k+1)) may not have landed yet
