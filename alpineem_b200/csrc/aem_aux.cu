@@ -331,12 +331,24 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
 // goes to U/W once per batch, one global atomic per non-zero bin, scaled by
 // fac and the image-pass sign.
 constexpr int FF_STRIP = 8;
+// add (a, b) to a shared (U1, U2) or (W1, W2) bin pair with one 64-bit
+// compare-and-swap (a float atomic add to shared memory is such a loop per
+// value; the two components of a pair always share their bin)
+__device__ __forceinline__ void hadd2(float2* p, float a, float b) {
+    unsigned long long* q = reinterpret_cast<unsigned long long*>(p);
+    unsigned long long old = *q, assumed;
+    do {
+        assumed = old;
+        const float x = __uint_as_float((unsigned)assumed) + a;
+        const float y = __uint_as_float((unsigned)(assumed >> 32)) + b;
+        old = atomicCAS(q, assumed, (unsigned long long)__float_as_uint(x) | ((unsigned long long)__float_as_uint(y) << 32));
+    } while (old != assumed);
+}
 // one lane's walk over a strip for one angle, in increasing delay (REV:
 // from the strip's end); see k_ff_bin_batch
 template <bool REV>
 __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw, float tf0, int w0, float fn, float fnh,
-                                        float* hist, int oU1, int oU2, int oW1, int oW2, int lo_ok, int hi_ok,
-                                        int& bad) {
+                                        float2* hist, int oU, int oW, int lo_ok, int hi_ok, int& bad) {
     int kU = INT_MIN, kW = INT_MIN;
     float u1l = 0.0f, u1h = 0.0f, u2l = 0.0f, u2h = 0.0f, w1l = 0.0f, w1h = 0.0f, w2l = 0.0f, w2h = 0.0f;
 #pragma unroll
@@ -352,13 +364,11 @@ __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw,
         if (iu != kU) {
             if (kU != INT_MIN) {
                 if (kU >= lo_ok && kU <= hi_ok) {
-                    atomicAdd(&hist[oU1 + kU - 1], u1l);
-                    atomicAdd(&hist[oU2 + kU - 1], u2l);
+                    hadd2(&hist[oU + kU - 1], u1l, u2l);
                     if (iu == kU + 1) {  // the high bin continues as the next low bin
                         u1l = u1h; u2l = u2h;
                     } else {
-                        atomicAdd(&hist[oU1 + kU], u1h);
-                        atomicAdd(&hist[oU2 + kU], u2h);
+                        hadd2(&hist[oU + kU], u1h, u2h);
                         u1l = u2l = 0.0f;
                     }
                 } else {
@@ -371,13 +381,11 @@ __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw,
         if (iw != kW) {
             if (kW != INT_MIN) {
                 if (kW >= lo_ok && kW <= hi_ok) {
-                    atomicAdd(&hist[oW1 + kW - 1], w1l);
-                    atomicAdd(&hist[oW2 + kW - 1], w2l);
+                    hadd2(&hist[oW + kW - 1], w1l, w2l);
                     if (iw == kW + 1) {
                         w1l = w1h; w2l = w2h;
                     } else {
-                        atomicAdd(&hist[oW1 + kW], w1h);
-                        atomicAdd(&hist[oW2 + kW], w2h);
+                        hadd2(&hist[oW + kW], w1h, w2h);
                         w1l = w2l = 0.0f;
                     }
                 } else {
@@ -393,19 +401,20 @@ __device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw,
         w2l = fmaf(1.0f - ww, d[j][3], w2l); w2h = fmaf(ww, d[j][3], w2h);
     }
     if (kU >= lo_ok && kU <= hi_ok) {
-        atomicAdd(&hist[oU1 + kU - 1], u1l); atomicAdd(&hist[oU1 + kU], u1h);
-        atomicAdd(&hist[oU2 + kU - 1], u2l); atomicAdd(&hist[oU2 + kU], u2h);
+        hadd2(&hist[oU + kU - 1], u1l, u2l);
+        hadd2(&hist[oU + kU], u1h, u2h);
     } else bad++;
     if (kW >= lo_ok && kW <= hi_ok) {
-        atomicAdd(&hist[oW1 + kW - 1], w1l); atomicAdd(&hist[oW1 + kW], w1h);
-        atomicAdd(&hist[oW2 + kW - 1], w2l); atomicAdd(&hist[oW2 + kW], w2h);
+        hadd2(&hist[oW + kW - 1], w1l, w2l);
+        hadd2(&hist[oW + kW], w1h, w2h);
     } else bad++;
 }
 
 __global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__ AemParams P,
                                                          const __grid_constant__ FarFieldDev F, int n0, int nt) {
     if (P.dstep) n0 = *P.dstep - nt + 1;  // graph replay: the batch ends at the current step
-    extern __shared__ float hist[];  // [group][4][hspan]: U1, U2, W1, W2
+    extern __shared__ float hist[];  // [group][U, W][hspan][2]: (U1, U2) and (W1, W2) pairs per bin
+    float2* hist2 = reinterpret_cast<float2*>(hist);
     __shared__ float ksh[64][3];
     __shared__ int bsh[64], vash[64];
     const int G = F.group, HS = F.hspan;
@@ -462,13 +471,14 @@ __global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__
             const float kw = walk_v ? Kv : Ku;
             const float tf0 = walk_v ? fmaf(Ku, (float)us, K0) : fmaf(Kv, (float)vs, K0);
             const int w0 = walk_v ? vs : us;
-            // histogram offsets: bin k of component m of angle g is hist[(4g+m)HS + k - bsh[g]]
-            const int oU1 = g * 4 * HS - bsh[g], oU2 = oU1 + HS, oW1 = oU1 + 2 * HS, oW2 = oU1 + 3 * HS;
+            // histogram offsets: the U pair of bin k of angle g is hist2[2g HS + k - bsh[g]],
+            // the W pair HS pairs further
+            const int oU = g * 2 * HS - bsh[g], oW = oU + HS;
             const int lo_ok = bsh[g] + 1, hi_ok = bsh[g] + HS - 1;
             if (kw >= 0.0f)
-                ff_walk<false>(d, kw, tf0, w0, fn, fnh, hist, oU1, oU2, oW1, oW2, lo_ok, hi_ok, bad);
+                ff_walk<false>(d, kw, tf0, w0, fn, fnh, hist2, oU, oW, lo_ok, hi_ok, bad);
             else
-                ff_walk<true>(d, kw, tf0, w0, fn, fnh, hist, oU1, oU2, oW1, oW2, lo_ok, hi_ok, bad);
+                ff_walk<true>(d, kw, tf0, w0, fn, fnh, hist2, oU, oW, lo_ok, hi_ok, bad);
         }
     }
     if (bad) atomicAdd(F.err, bad);
@@ -480,7 +490,8 @@ __global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__
     for (int e = tid; e < ng * 4 * HS; e += blockDim.x) {
         const float h = hist[e];
         if (h == 0.0f) continue;
-        const int g = e / (4 * HS), m = (e / HS) & 3, k = e % HS;
+        // e = ((g * 2 + half) * HS + k) * 2 + comp; m = 0 U1, 1 U2, 2 W1, 3 W2
+        const int g = e / (4 * HS), r = e % (4 * HS), m = (r / (2 * HS)) * 2 + (r & 1), k = (r % (2 * HS)) >> 1;
         const int va = vash[g], ang = va % F.nang, pass = va / F.nang;
         const long long gi = (long long)bsh[g] + k;
         if (gi < 0 || gi >= F.len) { atomicAdd(F.err, 1); continue; }
