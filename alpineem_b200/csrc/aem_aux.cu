@@ -595,6 +595,36 @@ __global__ void k_video(const __grid_constant__ AemParams P, const __grid_consta
     if (counter < steps) { at<T>(D.vid[1], o1) = hx; at<T>(D.vid[3], o1) = hy; at<T>(D.vid[5], o1) = hz; }
 }
 
+// Full-field export, ref :6960-7003: cell-centred averages of all six
+// components over i = 1..X-1-pbc_x, j = 1..Y-1-pbc_y, k = 1..Z-1-pbc_z (E at
+// the step, H half a step earlier, as the reference writes them), stored
+// component-major, i fastest: out[comp][k][j][i] in the reference's order
+// Ex, Ey, Ez, Hx, Hy, Hz.  Sums left to right as in the Fortran expression;
+// the divisions by 4 and 2 are exact.
+template <typename T>
+__global__ void k_full(const __grid_constant__ AemParams P, void* out, int n1, int n2, int n3) {
+    const long long n = (long long)n1 * n2 * n3;
+    const void *Ex = P.E[0], *Ey = P.E[1], *Ez = P.E[2], *Hx = P.H[0], *Hy = P.H[1], *Hz = P.H[2];
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % n1) + 1, j = (int)((q / n1) % n2) + 1, k = (int)(q / ((long long)n1 * n2)) + 1;
+        at<T>(out, q) = (fget<T>(P, Ex, i, j, k) + fget<T>(P, Ex, i, j + 1, k) + fget<T>(P, Ex, i, j, k + 1) + fget<T>(P, Ex, i, j + 1, k + 1)) / 4.0f;
+        at<T>(out, q + n) = (fget<T>(P, Ey, i, j, k) + fget<T>(P, Ey, i + 1, j, k) + fget<T>(P, Ey, i, j, k + 1) + fget<T>(P, Ey, i + 1, j, k + 1)) / 4.0f;
+        at<T>(out, q + 2 * n) = (fget<T>(P, Ez, i, j, k) + fget<T>(P, Ez, i + 1, j, k) + fget<T>(P, Ez, i, j + 1, k) + fget<T>(P, Ez, i + 1, j + 1, k)) / 4.0f;
+        at<T>(out, q + 3 * n) = (fget<T>(P, Hx, i, j, k) + fget<T>(P, Hx, i + 1, j, k)) / 2.0f;
+        at<T>(out, q + 4 * n) = (fget<T>(P, Hy, i, j, k) + fget<T>(P, Hy, i, j + 1, k)) / 2.0f;
+        at<T>(out, q + 5 * n) = (fget<T>(P, Hz, i, j, k) + fget<T>(P, Hz, i, j, k + 1)) / 2.0f;
+    }
+}
+
+int launch_full(const AemParams& P, void* out, const int n[3], cudaStream_t s) {
+    const long long cells = (long long)n[0] * n[1] * n[2];
+    if (cells <= 0) return 0;
+    const int blocks = (int)((cells + 255) / 256 < 148 * 8 ? (cells + 255) / 256 : 148 * 8);
+    if (P.kmax) k_full<cf><<<blocks, 256, 0, s>>>(P, out, n[0], n[1], n[2]);
+    else k_full<float><<<blocks, 256, 0, s>>>(P, out, n[0], n[1], n[2]);
+    return 1;
+}
+
 // ---------------------------------------------------------------------------
 // graph replay: the step counter advances once at the end of every step
 __global__ void k_step_advance(int* d) { *d += 1; }

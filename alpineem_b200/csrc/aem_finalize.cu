@@ -57,6 +57,7 @@ void Solver::finalize_and_write() {
     const bool K = d.kmax;
     const int T = d.steps;
     flush_farfield(done_);
+    full_flush();
     AEM_CUDA(cudaStreamSynchronize(stream_));
     const float mu0 = 1.25663706E-6f, ep0 = 8.85418782E-12f, c0 = 299792458.0f, pi = 3.14159265358979323846f;
     if (FF_.err) {

@@ -97,6 +97,8 @@ bool yee_fused_ok(const AemParams& P, int gridded_ports);
 int launch_yee(const AemParams& P, cudaStream_t s);
 int launch_yee4(const AemParams& P, cudaStream_t s);  // aem_yee4.cu (no x/y periodicity)
 int launch_taps(const AemParams& P, const TapDev& T, const FarFieldDev& F, int counter, int steps, cudaStream_t s);
+// full-field export of one step into `out` (6 x n0*n1*n2 values)
+int launch_full(const AemParams& P, void* out, const int n[3], cudaStream_t s);
 int launch_step_advance(int* d, cudaStream_t s);  // aem_aux.cu: *d += 1 (graph replay)
 
 }  // namespace aem

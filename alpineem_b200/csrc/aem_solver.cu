@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -83,6 +84,7 @@ void Solver::init() {
         setup_ports();
         setup_farfield();
         setup_taps();
+        setup_full();
         setup_fused();
         AEM_CUDA(cudaStreamSynchronize(stream_));
     } catch (...) {
@@ -128,6 +130,26 @@ void Solver::setup_fused() {
 
 void Solver::release() {
     if (stream_) cudaStreamSynchronize(stream_);
+    // steps already run still reach the export files (nothing is written if
+    // the device is in an error state)
+    try {
+        full_flush();
+    } catch (...) {
+    }
+    for (int q = 0; q < 6; q++) {
+        if (full_.f[q]) std::fclose(full_.f[q]);
+        full_.f[q] = nullptr;
+    }
+    for (int b = 0; b < 2; b++) {
+        if (full_.host[b]) cudaFreeHost(full_.host[b]);
+        if (full_.made[b]) cudaEventDestroy(full_.made[b]);
+        if (full_.copied[b]) cudaEventDestroy(full_.copied[b]);
+        full_.host[b] = nullptr;
+        full_.made[b] = full_.copied[b] = nullptr;
+        full_.pending[b] = 0;
+    }
+    if (full_.copy) cudaStreamDestroy(full_.copy);
+    full_.copy = nullptr;
     release_graph();
     for (void* p : bufs_) cudaFree(p);
     bufs_.clear();
@@ -569,6 +591,76 @@ void Solver::setup_taps() {
     }
 }
 
+// Full-field export files, opened at setup like the reference's units
+// 17-22 (ref :3971 allocation, :6995-7000 writes); one Fortran unformatted
+// record (4-byte length, FP32 values (re, im pairs for kmax), 4-byte
+// length) per component per step.
+void Solver::setup_full() {
+    const Deck& d = m_.d;
+    if (d.export_all != "yes") return;
+    const int N[3] = {d.X, d.Y, d.Z};
+    size_t cells = 1;
+    for (int a = 0; a < 3; a++) {
+        full_.n[a] = N[a] - 1 - d.pbc[a];
+        cells *= (size_t)full_.n[a];
+    }
+    if (cells * es_ > 0x7fffffffu)
+        throw std::invalid_argument("full-field export: one component of one step exceeds the 2 GiB record length");
+    full_.bytes = 6 * cells * es_;
+    AEM_CUDA(cudaStreamCreateWithFlags(&full_.copy, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+        full_.dev[b] = alloc(full_.bytes);
+        AEM_CUDA(cudaMallocHost(&full_.host[b], full_.bytes));
+        AEM_CUDA(cudaEventCreateWithFlags(&full_.made[b], cudaEventDisableTiming));
+        AEM_CUDA(cudaEventCreateWithFlags(&full_.copied[b], cudaEventDisableTiming));
+    }
+    static const char* nm[6] = {"Ex", "Ey", "Ez", "Hx", "Hy", "Hz"};
+    const std::string base = d.filename.substr(0, d.filename.size() >= 4 ? d.filename.size() - 4 : 0);
+    for (int q = 0; q < 6; q++) {
+        const std::string fn = (outdir_.empty() ? "" : outdir_ + "/") + base + "_full_" + nm[q] + ".bin";
+        full_.f[q] = std::fopen(fn.c_str(), "wb");
+        if (!full_.f[q]) throw std::runtime_error("full-field export: cannot open " + fn);
+    }
+}
+
+// average step `counter` into staging buffer counter % 2 and start its copy
+// to the host; the buffer's previous step (counter - 2) is written first
+void Solver::full_tap(int counter) {
+    const int b = counter & 1;
+    if (full_.pending[b]) full_drain(b);
+    phase(AEM_PHASE_TAPS, [&] { return launch_full(P_, full_.dev[b], full_.n, stream_); });
+    AEM_CUDA(cudaEventRecord(full_.made[b], stream_));
+    AEM_CUDA(cudaStreamWaitEvent(full_.copy, full_.made[b], 0));
+    AEM_CUDA(cudaMemcpyAsync(full_.host[b], full_.dev[b], full_.bytes, cudaMemcpyDeviceToHost, full_.copy));
+    AEM_CUDA(cudaEventRecord(full_.copied[b], full_.copy));
+    full_.pending[b] = counter;
+    d2h_bytes_ += full_.bytes;
+}
+
+// wait for buffer b's copy and append its six records to the files
+void Solver::full_drain(int b) {
+    AEM_CUDA(cudaEventSynchronize(full_.copied[b]));
+    const size_t per = full_.bytes / 6;
+    const int32_t L = (int32_t)per;
+    for (int q = 0; q < 6; q++) {
+        std::FILE* f = full_.f[q];
+        if (std::fwrite(&L, 4, 1, f) != 1 || std::fwrite((const char*)full_.host[b] + q * per, 1, per, f) != per ||
+            std::fwrite(&L, 4, 1, f) != 1)
+            throw std::runtime_error("full-field export: write failed");
+    }
+    full_.pending[b] = 0;
+}
+
+// write every step still held in a copy buffer, oldest first
+void Solver::full_flush() {
+    if (!full_.f[0]) return;
+    int first = 0;
+    if (full_.pending[1] && (!full_.pending[0] || full_.pending[1] < full_.pending[0])) first = 1;
+    for (int b : {first, 1 - first})
+        if (full_.pending[b]) full_drain(b);
+    for (std::FILE* f : full_.f) std::fflush(f);
+}
+
 // run one launcher; with profiling on, bracket it with events on the stream
 template <typename Fn>
 void Solver::phase(int ph, Fn&& fn) {
@@ -678,6 +770,7 @@ void Solver::step(int counter) {
         phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin(P_, FF_, counter, stream_); });
     }
     phase(AEM_PHASE_TAPS, [&] { return launch_taps(P_, TP_, FF_, counter, m_.d.steps, stream_); });
+    if (full_.f[0]) full_tap(counter);
 }
 
 // bin the steps ff_n0_..last held in the difference buffer
@@ -696,7 +789,10 @@ void Solver::run(int n) {
     }
     // the last step bins whatever the batch buffer still holds; earlier
     // partial batches wait for more steps (or for flush())
-    if (done_ == m_.d.steps) flush_farfield(done_);
+    if (done_ == m_.d.steps) {
+        flush_farfield(done_);
+        full_flush();
+    }
     AEM_CUDA(cudaGetLastError());
 }
 
@@ -708,6 +804,7 @@ void Solver::release_graph() {
 
 bool Solver::graph_ready(int g) const {
     if (g < 1 || done_ == 0 || done_ + g > m_.d.steps) return false;  // the first step runs eagerly
+    if (full_.f[0]) return false;                                       // the host writes every step's export
     if (fused_ && (g & 1)) return false;                                // an even number of buffer swaps
     if (FF_.tb > 1 && (g % FF_.tb != 0 || ff_n0_ != done_ + 1)) return false;  // whole far-field batches
     return true;

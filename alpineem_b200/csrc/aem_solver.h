@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -98,9 +99,13 @@ class Solver {
     void setup_farfield();
     void setup_taps();
     void setup_fused();
+    void setup_full();
     void step(int counter);
     void flush_farfield(int last);
     bool graph_ready(int g) const;  // can a g-step graph chunk start at the next step?
+    void full_tap(int counter);
+    void full_drain(int b);
+    void full_flush();
     void capture_graph(int g);
     void release_graph();
     template <typename Fn>
@@ -138,6 +143,21 @@ class Solver {
     // graph replay
     int* dstep_ = nullptr;          // device step counter
     cudaGraphExec_t graph_ = nullptr;
+    // full-field export (every step's averaged fields to <name>_full_*.bin):
+    // the averages go to a device staging buffer, a second stream copies
+    // them to pinned host memory, and the host writes them to the files two
+    // steps later; two buffers of each, so the copy and the file write of
+    // one step overlap the kernels of the next
+    struct FullExport {
+        int n[3] = {0, 0, 0};      // averaged cells along x, y, z
+        size_t bytes = 0;          // one step, six components
+        void* dev[2] = {nullptr, nullptr};
+        void* host[2] = {nullptr, nullptr};
+        cudaEvent_t made[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+        int pending[2] = {0, 0};   // step whose copy buffer b holds (0: none)
+        std::FILE* f[6] = {};
+        cudaStream_t copy = nullptr;
+    } full_;
     int graph_g_ = 0;               // steps per graph
     long long graph_launches_ = 0;  // kernels per replay
 };

@@ -54,6 +54,16 @@ DECKS = {
     "video": dict(n=(32, 31, 30), steps=100, f="25E9", excitation=("plane wave", 1, 0, 60, 120, 45),
                   video=("y", 15), mats=[("simple", 2, (3, 3, 3), (0, 0, 0))],
                   objects=[("cylinder", 2, "z", (16, 15, 12), (6, 3))]),
+    # every step's cell-averaged fields exported (<name>_full_*.bin): a
+    # dipole on the fused kernel and a constant-k unit cell (complex records)
+    "full_dipole": dict(n=(26, 24, 22), steps=90, f="15E9", pulse=1, excitation=("antenna", 1, 0, 1), full="yes",
+                        mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (3, 3, 3), (0.01, 0, 0))],
+                        objects=[("block", 4, (13, 12, 7), (1, 1, 5)), ("block", 4, (13, 12, 13), (1, 1, 5)),
+                                 ("sphere", 5, (6, 7, 11), 3)],
+                        ports=[("basic", "z", 50, (13, 12, 12), (1, 1, 1))]),
+    "full_kmax": dict(kmax=True, n=(28, 6, 8), dl=("0.25E-3", "0.25E-3", "0.25E-3"), steps=150, f="8E9",
+                      bc=(0, 0, 1, 1, 1, 1), excitation=("plane wave", 1, 0, "TE", "+"), k=("200.0", "100.0"), full="yes",
+                      mats=[("simple", 5, (4, 4, 4), (0, 0, 0))], objects=[("block", 5, (10, 1, 1), (6, 6, 8))]),
     # constant-k periodic solver, TE and TM, oblique k in the y,z plane
     "kmax_te": dict(kmax=True, n=(36, 10, 10), dl=("0.25E-3", "0.25E-3", "0.25E-3"), steps=300, f="8E9", bc=(0, 0, 1, 1, 1, 1),
                     excitation=("plane wave", 1, 0, "TE", "+"), k=("300.0", "150.0"),
