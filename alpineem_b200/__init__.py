@@ -77,6 +77,18 @@ def load_library():
                             ctypes.c_void_p, ctypes.c_void_p]
     lib.aem_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]
     lib.aem_transfer_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    i3 = ctypes.c_int * 3
+    lib.aem_design_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i3, i3, ctypes.c_int, ctypes.POINTER(h)]
+    lib.aem_design_set_probe.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    lib.aem_design_set_eps.argtypes = [h, ctypes.c_void_p, ctypes.c_void_p]
+    lib.aem_design_forward.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.aem_design_gradient.argtypes = [h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+    lib.aem_design_timing.argtypes = [h, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+    lib.aem_design_get_field.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
+    lib.aem_design_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]
+    lib.aem_design_last_error.argtypes = [h]
+    lib.aem_design_last_error.restype = ctypes.c_char_p
+    lib.aem_design_destroy.argtypes = [h]
     _lib = lib
     return lib
 

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "../../include/alpineem_b200.h"
+#include "aem_design.h"
 #include "aem_dft.h"
 #include "aem_solver.h"
 
@@ -315,6 +316,108 @@ const char* aem_last_error(aem_handle* h) { return h ? h->err.c_str() : g_create
 
 int aem_destroy(aem_handle* h) {
     delete h;
+    return AEM_OK;
+}
+
+}  // extern "C"
+
+struct aem_design {
+    std::unique_ptr<aem::DesignRun> r;
+    std::string err;
+};
+
+namespace {
+template <typename F>
+int dguard(aem_design* d, F&& f) {
+    try {
+        return f();
+    } catch (const aem::DeckError& e) {
+        (d ? d->err : g_create_err) = e.what();
+        return AEM_ERR_INPUT;
+    } catch (const std::invalid_argument& e) {
+        (d ? d->err : g_create_err) = e.what();
+        return AEM_ERR_ARG;
+    } catch (const std::exception& e) {
+        std::string m = e.what();
+        (d ? d->err : g_create_err) = m;
+        return m.rfind("CUDA", 0) == 0 ? AEM_ERR_CUDA : AEM_ERR_INPUT;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int aem_design_create(const char* inputs_path, const char* outdir, const int lo[3], const int n[3], int precision,
+                      aem_design** out) {
+    if (!inputs_path || !lo || !n || !out) return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    *out = nullptr;
+    if (int rc = need_device()) return rc;
+    return dguard(nullptr, [&]() {
+        auto d = std::make_unique<aem_design>();
+        d->r.reset(aem::DesignRun::create(inputs_path, outdir ? outdir : "", lo, n, precision));
+        *out = d.release();
+        return AEM_OK;
+    });
+}
+
+int aem_design_set_probe(aem_design* d, int comp, int i, int j, int k, double freq_hz) {
+    if (!d) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        d->r->set_probe(comp, i, j, k, freq_hz);
+        return AEM_OK;
+    });
+}
+
+int aem_design_set_eps(aem_design* d, const float* eps, const float* sigma) {
+    if (!d) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        d->r->set_design(eps, sigma);
+        return AEM_OK;
+    });
+}
+
+int aem_design_forward(aem_design* d, int checkpoint_every, double* fom, double dft[2]) {
+    if (!d || !fom) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        *fom = d->r->forward(checkpoint_every, dft);
+        return AEM_OK;
+    });
+}
+
+int aem_design_gradient(aem_design* d, float* grad_eps, float* grad_sigma, double scale) {
+    if (!d) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        d->r->gradient(grad_eps, grad_sigma, scale);
+        return AEM_OK;
+    });
+}
+
+int aem_design_timing(aem_design* d, double ms[2], long long launches[2]) {
+    if (!d || !ms || !launches) return AEM_ERR_ARG;
+    d->r->timing(ms, launches);
+    return AEM_OK;
+}
+
+int aem_design_get_field(aem_design* d, int comp, int dims[3], double* out) {
+    if (!d || !dims) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        std::vector<double> v;
+        d->r->get_field(comp, v, dims);
+        if (out) std::memcpy(out, v.data(), v.size() * sizeof(double));
+        return AEM_OK;
+    });
+}
+
+int aem_design_stream(aem_design* d, void** stream) {
+    if (!d || !stream) return AEM_ERR_ARG;
+    *stream = d->r->stream();
+    return AEM_OK;
+}
+
+const char* aem_design_last_error(aem_design* d) { return d ? d->err.c_str() : g_create_err.c_str(); }
+
+int aem_design_destroy(aem_design* d) {
+    delete d;
     return AEM_OK;
 }
 

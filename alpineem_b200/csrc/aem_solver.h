@@ -51,6 +51,12 @@ class Solver {
     void get_field(int comp, std::vector<double>& re, std::vector<double>& im, int dims[3]);
 
     const Deck& deck() const { return m_.d; }
+    // device constants, ports and host model (read by the design-gradient
+    // engine, which runs its own state over the same grid)
+    const AemParams& params() const { return P_; }
+    const PortSet& ports() const { return PS_; }
+    const HostModel& model() const { return m_; }
+    bool port_in_cpml() const { return split_; }
     const std::vector<float>& geometry() const { return m_.geometry; }
     int steps_done() const { return done_; }
     size_t device_bytes() const { return dev_bytes_; }

@@ -108,3 +108,35 @@ def kmax_batch(n_inst=64, steps=6000, seed=3, dl="1E-3", f="10E9", nxy=64, depth
                  sheets=[("z", 3, z0 + depth, (a, b), (sa, sb)) for a, b, sa, sb in sheets])
         decks_.append(d)
     return decks_
+
+
+def adjoint_probe(n=192, steps=3000, design=(64, 64, 32), seed=4, pml_cells=12, dl="1E-3", f="20E9",
+                  freq=10e9, gap=40, arm=10, port_z=None):
+    """Design-gradient workload: an n^3 grid (spacing dl, `pml_cells` of
+    CPML on every face) driven by a z-directed 1-cell 50-ohm lumped port
+    (Gaussian pulse) between two 1x1x`arm` PEC arms near the -z side, a
+    design box of `design` cells (x, y, z) centred in x and y above it whose
+    eps_r is drawn from U[1, 4] (numpy default_rng(seed)), and an Ez probe
+    `gap` cells beyond the box's +z face on the axis.  The figure of merit is
+    |DFT of the probe at `freq`|^2.
+
+    Returns (deck, ext_text, lo, n, probe, freq, eps) with eps of shape
+    (nz, ny, nx) float32 and probe = (comp, i, j, k)."""
+    rng = np.random.default_rng(seed)
+    c = n // 2
+    nx, ny, nz = design
+    lo = (c - nx // 2 + 1, c - ny // 2 + 1, 0)
+    pz = port_z if port_z is not None else pml_cells + arm + 8
+    z0 = pz + arm + 1 + max(4, (n - 2 * pml_cells - nz - gap) // 4 - arm)
+    lo = (lo[0], lo[1], z0)
+    probe = (2, c, c, z0 + nz - 1 + gap)
+    if probe[3] >= n + 1 - pml_cells - 1:
+        raise ValueError("the probe falls into the CPML; enlarge n or shrink the gap")
+    eps = rng.uniform(1.0, 4.0, size=(nz, ny, nx)).astype(np.float32)
+    d = dict(n=(n, n, n), dl=(dl, dl, dl), steps=steps, factor=1, f=f, pulse=1, bc=(0, 0, 0, 0, 0, 0),
+             excitation=("antenna", 1, 0, 1), name="data.dat",
+             mats=[("simple", 1, (1, 1, 1), ("1E8", "1E8", "1E8"))],
+             objects=[("block", 1, (c, c, pz - arm), (1, 1, arm)), ("block", 1, (c, c, pz + 1), (1, 1, arm))],
+             ports=[("basic", "z", 50, (c, c, pz), (1, 1, 1))])
+    ext = "pml_cells %d\ngeometry_bin no\n" % pml_cells
+    return d, ext, lo, design, probe, float(freq), eps

@@ -57,6 +57,12 @@ def parse_args():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched kmax-instance measurement")
     ap.add_argument("--batch-steps", type=int, default=192, help="timed steps of every batched instance")
     ap.add_argument("--batch-graph", type=int, default=32, help="steps per captured CUDA graph")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the design-gradient measurement")
+    ap.add_argument("--adjoint-n", type=int, default=192, help="grid cells per axis of the design-gradient workload")
+    ap.add_argument("--adjoint-steps", type=int, default=3000)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=200, help="steps between forward checkpoints")
+    ap.add_argument("--adjoint-fd", type=int, default=0,
+                    help="design cells checked against FP64 central differences (2 FP64 runs each)")
     return ap.parse_args()
 
 
@@ -244,6 +250,75 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
             "batched_mcell_updates_per_s": round(world * cells * steps / bat / 1e6, 1)}
 
 
+def adjoint_gradient(args, max_over_ranks):
+    """Design gradient (workloads.adjoint_probe: 192^3, 12-cell CPML, 3000
+    steps, 64x64x32 design cells of eps_r ~ U[1,4], |DFT_10GHz(Ez)|^2 at a
+    probe 40 cells beyond the box): device time of a plain FP32 forward run
+    against the checkpointed forward run plus the adjoint sweep (which
+    recomputes every checkpoint segment but the last), and the same with
+    the whole design-box history kept (one segment).  With --adjoint-fd C,
+    C random design cells are checked against FP64 central differences
+    (delta = 1e-3).  Every rank runs its own replica."""
+    import numpy as np
+    from alpineem_b200 import workloads
+    from alpineem_b200.adjoint import Design
+    from alpineem_b200.deck import deck_text
+
+    n, steps, K = args.adjoint_n, args.adjoint_steps, args.adjoint_checkpoint
+    d, ext, lo, box, probe, freq, eps = workloads.adjoint_probe(n=n, steps=steps)
+    tmp = tempfile.mkdtemp(prefix="aem_adj_")
+    path = os.path.join(tmp, "inputs.txt")
+    with open(path, "w") as f:
+        f.write(deck_text(d))
+    with open(path + ".b200", "w") as f:
+        f.write(ext)
+    out = {"workload": "adjoint_probe", "grid": [n] * 3, "cpml_cells": 12, "steps": steps,
+           "design_box": list(box), "design_cells": int(np.prod(box)), "probe": list(probe), "freq_hz": freq,
+           "figure_of_merit": "|DFT of Ez at the probe|^2", "dtype": "f32", "checkpoint_every": K}
+    with Design(path, lo, box, probe, freq, precision=32) as dsn:
+        dsn.set_design(eps)
+        dsn.forward(0)  # warm-up
+        f_plain, _ = dsn.forward(0)
+        t_plain = dsn.timing()[0]
+        f_ck, _ = dsn.forward(K)
+        g = dsn.gradient()
+        t_fwd, t_grad, l_fwd, l_grad = dsn.timing()
+        dsn.forward(steps)
+        g_all = dsn.gradient()
+        t_fwd_all, t_grad_all, _, _ = dsn.timing()
+        cells = n ** 3
+        t_plain, t_fwd, t_grad = max_over_ranks(t_plain), max_over_ranks(t_fwd), max_over_ranks(t_grad)
+        t_fwd_all, t_grad_all = max_over_ranks(t_fwd_all), max_over_ranks(t_grad_all)
+        out.update({"fom": f_plain, "plain_forward_ms": round(t_plain, 2),
+                    "forward_mcell_updates_per_s": round(cells * steps / (t_plain / 1e3) / 1e6, 1),
+                    "checkpointed_forward_ms": round(t_fwd, 2), "gradient_ms": round(t_grad, 2),
+                    "ratio": round((t_fwd + t_grad) / t_plain, 3),
+                    "store_all_forward_ms": round(t_fwd_all, 2), "store_all_gradient_ms": round(t_grad_all, 2),
+                    "store_all_ratio": round((t_fwd_all + t_grad_all) / t_plain, 3),
+                    "gradient_launches": l_grad, "forward_launches": l_fwd,
+                    "segments_equal": bool(np.array_equal(g, g_all)), "fom_equal": f_plain == f_ck,
+                    "grad_abs_max": float(np.abs(g).max())})
+    if args.adjoint_fd > 0:
+        rng = np.random.default_rng(7)
+        pick = [tuple(int(rng.integers(0, s)) for s in eps.shape) for _ in range(args.adjoint_fd)]
+        errs = []
+        with Design(path, lo, box, probe, freq, precision=64) as d64:
+            for c in pick:
+                vals, pts = [], []
+                for sgn in (1, -1):
+                    e = eps.copy()
+                    e[c] = np.float32(float(e[c]) + sgn * 1e-3)
+                    pts.append(float(e[c]))
+                    d64.set_design(e)
+                    vals.append(d64.forward(0)[0])
+                fd = (vals[0] - vals[1]) / (pts[0] - pts[1])
+                errs.append({"cell": list(c), "fd": fd, "adjoint_f32": float(g[c]),
+                             "rel_err": abs(float(g[c]) - fd) / abs(fd) if fd else None})
+        out["fd_check"] = {"delta": 1e-3, "fd_precision": "f64", "cells": errs,
+                           "max_rel_err": max(e["rel_err"] for e in errs if e["rel_err"] is not None)}
+    return out
+
+
 def ours(args):
     import torch
     import alpineem_b200 as ab
@@ -351,6 +426,10 @@ def ours(args):
     if not args.no_batch:
         batched = batched_kmax(rank, world, args.batch_steps, args.batch_graph, barrier, max_over_ranks)
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_gradient(args, max_over_ranks)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, threads, ccells = oracle_sample(args.cpu_n, 1, args.cpu_steps)
@@ -369,7 +448,7 @@ def ours(args):
                            "parallelism": "replicas" if world > 1 else "single"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": launches, "phases_ms_per_step": phases, "far_field": far_field,
-                "batched_kmax": batched,
+                "batched_kmax": batched, "adjoint": adjoint,
                 "setup_s": round(t_setup, 2), "workload_gen_s": round(t_gen, 2)}
         print(json.dumps(line), flush=True)
     if dist:

@@ -206,6 +206,63 @@ const char* aem_last_error(aem_handle* h);
 /* Free the handle and its device memory. */
 int aem_destroy(aem_handle* h);
 
+/* ---- design gradients -------------------------------------------------
+ * The reference optimises material values with two solver runs per
+ * iteration and a spectral overlap of their fields
+ * (optimization_scripts/adjoint_optimization/adjoint_optimization.py:55-134,
+ * the `fdtd.py` runs and the F1..F4 overlap).  These entry points return the
+ * exact gradient of the discrete time loop instead: a forward run of the
+ * deck with per-cell eps_r (and optionally sigma) inside a design box, then
+ * the transposed update backwards in time, recomputing each checkpoint
+ * segment.  Figure of merit F = |D|^2, D = sum_n c^n exp(-i 2 pi f n dt)
+ * over all steps n, c^n the probe E component after step n.
+ * Supported decks: standard solver, no periodic axes, lumped-port source
+ * (no plane wave), no sheets, Drude poles or gridded ports; the design box
+ * and the probe keep out of the CPML slabs and off the ports. */
+typedef struct aem_design aem_design;
+
+/* Build the run from the deck at `inputs_path`; the design box is cells
+ * lo..lo+n-1 (reference indices).  precision 4: FP32 state, the reference's
+ * arithmetic; 8: FP64 state (finite-difference checks). */
+int aem_design_create(const char* inputs_path, const char* outdir, const int lo[3], const int n[3], int precision,
+                      aem_design** out);
+
+/* Probe: E component comp (0 x, 1 y, 2 z) at reference edge (i, j, k) and the
+ * DFT frequency in Hz. */
+int aem_design_set_probe(aem_design* d, int comp, int i, int j, int k, double freq_hz);
+
+/* Design values per cell, n0*n1*n2 float32, x fastest; host or device
+ * pointers.  sigma NULL keeps the conductivity of the deck's materials. */
+int aem_design_set_eps(aem_design* d, const float* eps, const float* sigma);
+
+/* Forward run over the deck's steps.  checkpoint_every < 1: a plain run;
+ * otherwise the state is kept every that many steps for
+ * aem_design_gradient.  fom gets F, dft (may be NULL) gets D (re, im). */
+int aem_design_forward(aem_design* d, int checkpoint_every, double* fom, double dft[2]);
+
+/* scale * dF/d eps_r and scale * dF/d sigma per design cell (float32,
+ * x fastest, host or device pointers, either may be NULL).  Needs a
+ * checkpointed aem_design_forward since the last aem_design_set_eps. */
+int aem_design_gradient(aem_design* d, float* grad_eps, float* grad_sigma, double scale);
+
+/* Device time in ms of the last forward [0] and gradient [1] calls, and the
+ * kernels each launched. */
+int aem_design_timing(aem_design* d, double ms[2], long long launches[2]);
+
+/* Current field component comp (0..5 = Ex, Ey, Ez, Hx, Hy, Hz) of the run's
+ * forward state in the reference layout (as aem_get_field); dims gets its
+ * extents, out holds dims[0]*dims[1]*dims[2] values (NULL: dims only). */
+int aem_design_get_field(aem_design* d, int comp, int dims[3], double* out);
+
+/* The CUDA stream of the run (cudaStream_t). */
+int aem_design_stream(aem_design* d, void** stream);
+
+/* Message of the last failing call on d (of the last aem_design_create when
+ * d is NULL). */
+const char* aem_design_last_error(aem_design* d);
+
+int aem_design_destroy(aem_design* d);
+
 #ifdef __cplusplus
 }
 #endif
