@@ -19,9 +19,11 @@
 //   k_adj_h        E bulk + CPML E transposed, gathered onto H faces
 //   k_adj_ports_h  line currents and loop current transposed
 //   k_adj_e        H bulk + CPML H transposed, gathered onto E edges
-// Notation: lE, lH are the adjoints of E^n, H^{n-1/2}; w = Gb lE;
+// Notation: lE, lH are the adjoints of E^n, H^{n-1/2}.  The E-side state
+// kept is w = Gb lE (lE itself is needed only on design and port edges, as
+// w / Gb), so the adjoint moves as many bytes per step as the forward pass.
 // se = the adjoint of the E psi value just written (b-scaled psi adjoint plus
-// Gb lE), sh likewise for H (b se_next + DB lH).  The CPML, port and probe
+// w), sh likewise for H (b sh_next + DB lH).  The CPML, port and probe
 // edges never meet the design box or each other (checked on the host), which
 // lets each transposed operation sit in the kernel that owns its cells.
 #include <cuda_runtime.h>
@@ -55,7 +57,6 @@ struct DsnDev {
     R* H[3];
     R* pe[3][3][2];  // CPML psi, [component][slab axis][side]
     R* ph[3][3][2];
-    R* lE[3];
     R* lH[3];
     R* w[3];
     R* se[3][3][2];
@@ -109,19 +110,6 @@ __device__ __forceinline__ int dsn_edge_pos(const DsnDev<R>& D, long long q, int
     *py = D.eo[c][1] + (int)((r / D.en[c][0]) % D.en[c][1]);
     *pz = D.eo[c][2] + (int)(r / ((long long)D.en[c][0] * D.en[c][1]));
     return c;
-}
-
-// E component c updated by the bulk loop at this storage position (no
-// periodic axes): normal axis 1..N-1, tangential axes 2..N-1
-__device__ __forceinline__ bool e_upd(const AemParams& P, int c, int px, int py, int pz) {
-    const bool x = c == 0 ? (px >= 0 && px <= P.SX - 2) : (px >= 1 && px <= P.SX - 2);
-    const bool y = c == 1 ? (py >= 0 && py <= P.SY - 2) : (py >= 1 && py <= P.SY - 2);
-    const bool z = c == 2 ? (pz >= 0 && pz <= P.SZ - 2) : (pz >= 1 && pz <= P.SZ - 2);
-    return x && y && z;
-}
-// H faces updated: reference indices 1..N-1 on every axis
-__device__ __forceinline__ bool h_upd(const AemParams& P, int px, int py, int pz) {
-    return px >= 0 && py >= 0 && pz >= 0 && px <= P.SX - 2 && py <= P.SY - 2 && pz <= P.SZ - 2;
 }
 
 // Ga/Gb of E edge c: the design box's own values, else the solver's
@@ -211,8 +199,82 @@ __global__ void k_dsn_coef(const __grid_constant__ AemParams P, const __grid_con
 // forward
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_dsn_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
+__device__ __forceinline__ R ldg(const R* p) { return __ldg(p); }
+__device__ __forceinline__ int ldg_id(const uint8_t* p) { return (int)__ldg(p); }
+
+// Per-block copies of the small tables the volume kernels index per cell:
+// uniform-edge Ga/Gb and cell eps/sigma per material, CPML b/c per slab
+// depth.  Shared memory keeps the id -> coefficient lookup off the global
+// memory latency chain and serves divergent CPML depths in one access.
+struct DsnTabs {
+    float ga[AEM_MAX_MATERIALS][3], gb[AEM_MAX_MATERIALS][3];
+    float eps[AEM_MAX_MATERIALS][3], sig[AEM_MAX_MATERIALS][3];
+    float be[3][2][AEM_MAX_PML], ce[3][2][AEM_MAX_PML], bh[3][2][AEM_MAX_PML], ch[3][2][AEM_MAX_PML];
+};
+
+// fill the block's tables (every thread of the block must call it)
+__device__ inline void load_tabs(const AemParams& P, DsnTabs& T) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int q = tid; q < P.nmat * 3; q += nt) {
+        const int m = q / 3, c = q % 3;
+        T.ga[m][c] = P.ucoef[m].ga[c];
+        T.gb[m][c] = P.ucoef[m].gb[c];
+        T.eps[m][c] = P.mat[m].eps[c];
+        T.sig[m][c] = P.mat[m].sig[c];
+    }
+    for (int q = tid; q < 3 * 2 * AEM_MAX_PML; q += nt) {
+        const int a = q / (2 * AEM_MAX_PML), sd = (q / AEM_MAX_PML) % 2, d = q % AEM_MAX_PML;
+        if (d >= P.npml[a][sd]) continue;
+        T.be[a][sd][d] = P.be[a][sd][d];
+        T.ce[a][sd][d] = P.ce[a][sd][d];
+        T.bh[a][sd][d] = P.bh[a][sd][d];
+        T.ch[a][sd][d] = P.ch[a][sd][d];
+    }
+    __syncthreads();
+}
+
+// Ga/Gb of E component c from its four cell ids (ref order), as edge_coef
+template <typename R>
+__device__ __forceinline__ void coef1(const AemParams& P, const DsnTabs& T, int c, int i0, int i1, int i2, int i3, R& ga, R& gb) {
+    if (i0 == i1 && i0 == i2 && i0 == i3) {
+        ga = (R)T.ga[i0][c];
+        gb = (R)T.gb[i0][c];
+        return;
+    }
+    const float e = (T.eps[i0][c] + T.eps[i1][c] + T.eps[i2][c] + T.eps[i3][c]) / 4.0f;
+    const float s = (T.sig[i0][c] + T.sig[i1][c] + T.sig[i2][c] + T.sig[i3][c]) / 4.0f;
+    ga = (R)d_ga(s, e, P.dt);
+    gb = (R)d_gb(s, e, P.dt);
+}
+
+// Ga/Gb of the three E components at one position from the ids of the
+// cells (px,py), (px-1,py), (px,py-1), (px-1,py-1) in this plane (a) and the
+// plane below (b); unaveraged edges (index 1 on an axis) take vacuum.  The
+// design box's own values override (the caller).
+template <typename R>
+__device__ __forceinline__ void coef3(const AemParams& P, const DsnTabs& T, bool unavg, const int a[4], const int b[4], R ga[3], R gb[3]) {
+    const int z = unavg ? 0 : a[0];
+    if (unavg || (a[0] == a[1] && a[0] == a[2] && a[0] == a[3] && a[0] == b[0] && a[0] == b[1] && a[0] == b[2] && a[0] == b[3])) {
+        for (int c = 0; c < 3; c++) {
+            ga[c] = (R)T.ga[z][c];
+            gb[c] = (R)T.gb[z][c];
+        }
+        return;
+    }
+    coef1(P, T, 0, a[0], a[2], b[0], b[2], ga[0], gb[0]);
+    coef1(P, T, 1, a[0], a[1], b[0], b[1], ga[1], gb[1]);
+    coef1(P, T, 2, a[0], a[1], a[2], a[3], ga[2], gb[2]);
+}
+
+// Each thread marches one (x, y) column through DZCH planes; the values of
+// the plane below (E for H, H and cell ids for E) are carried in registers.
+// Read-only data goes through the non-coherent path so the loads of the
+// next plane can issue ahead of this plane's stores.
+template <typename R>
+__global__ void __launch_bounds__(256, 5) k_dsn_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
+    __shared__ DsnTabs T;
+    load_tabs(P, T);
     if (px > P.SX - 2 || py > P.SY - 2) return;
     const R *Ex = D.E[0], *Ey = D.E[1], *Ez = D.E[2];
     R *Hx = D.H[0], *Hy = D.H[1], *Hz = D.H[2];
@@ -220,77 +282,123 @@ __global__ void __launch_bounds__(256) k_dsn_h(const __grid_constant__ AemParams
     const float DB = P.DB, dhx = P.den_h[0][i - 1], dhy = P.den_h[1][j - 1];
     const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
     const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+    const bool colpml = qx_lo || qx_hi || qy_lo || qy_hi;
     const long long PX = P.PX, PL = P.plane;
-    const int pz_end = min(P.SZ - 2, ((int)blockIdx.z + 1) * DZCH - 1);
-    for (int pz = blockIdx.z * DZCH; pz <= pz_end; pz++) {
+    const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
+    long long c = lin(P, px, py, pz0);
+    R ex = ldg(Ex + c), ey = ldg(Ey + c);
+    for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
         const int k = pz + 1;
-        const long long c = lin(P, px, py, pz);
         const float dhz = P.den_h[2][k - 1];
-        const R ex = Ex[c], ey = Ey[c], ez = Ez[c];
-        const R ex_jp = Ex[c + PX], ex_kp = Ex[c + PL], ey_ip = Ey[c + 1], ey_kp = Ey[c + PL], ez_ip = Ez[c + 1], ez_jp = Ez[c + PX];
-        R hxv = Hx[c], hyv = Hy[c], hzv = Hz[c];
+        const R ez = ldg(Ez + c);
+        const R ex_jp = ldg(Ex + c + PX), ex_kp = ldg(Ex + c + PL), ey_ip = ldg(Ey + c + 1), ey_kp = ldg(Ey + c + PL);
+        const R ez_ip = ldg(Ez + c + 1), ez_jp = ldg(Ez + c + PX);
+        R hxv = ldg(Hx + c), hyv = ldg(Hy + c), hzv = ldg(Hz + c);
         hxv = hxv + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
         hyv = hyv + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
         hzv = hzv + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
         const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-        if (qy_lo) hxv = hxv + DB * dsn_psi<R>(D.ph[0][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-        if (qy_hi) hxv = hxv + DB * dsn_psi<R>(D.ph[0][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-        if (qz_lo) hxv = hxv + DB * dsn_psi<R>(D.ph[0][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-        if (qz_hi) hxv = hxv + DB * dsn_psi<R>(D.ph[0][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-        if (qx_lo) hyv = hyv + DB * dsn_psi<R>(D.ph[1][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-        if (qx_hi) hyv = hyv + DB * dsn_psi<R>(D.ph[1][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-        if (qz_lo) hyv = hyv + DB * dsn_psi<R>(D.ph[1][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-        if (qz_hi) hyv = hyv + DB * dsn_psi<R>(D.ph[1][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-        if (qx_lo) hzv = hzv + DB * dsn_psi<R>(D.ph[2][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-        if (qx_hi) hzv = hzv + DB * dsn_psi<R>(D.ph[2][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-        if (qy_lo) hzv = hzv + DB * dsn_psi<R>(D.ph[2][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-        if (qy_hi) hzv = hzv + DB * dsn_psi<R>(D.ph[2][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+        if (colpml || qz_lo || qz_hi) {
+            if (qy_lo) hxv = hxv + DB * dsn_psi<R>(D.ph[0][1][0], T.bh[1][0][qy_lo - 1], T.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hxv = hxv + DB * dsn_psi<R>(D.ph[0][1][1], T.bh[1][1][qy_hi - 1], T.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+            if (qz_lo) hxv = hxv + DB * dsn_psi<R>(D.ph[0][2][0], T.bh[2][0][qz_lo - 1], T.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hxv = hxv + DB * dsn_psi<R>(D.ph[0][2][1], T.bh[2][1][qz_hi - 1], T.ch[2][1][qz_hi - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hyv = hyv + DB * dsn_psi<R>(D.ph[1][0][0], T.bh[0][0][qx_lo - 1], T.ch[0][0][qx_lo - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hyv = hyv + DB * dsn_psi<R>(D.ph[1][0][1], T.bh[0][1][qx_hi - 1], T.ch[0][1][qx_hi - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qz_lo) hyv = hyv + DB * dsn_psi<R>(D.ph[1][2][0], T.bh[2][0][qz_lo - 1], T.ch[2][0][qz_lo - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hyv = hyv + DB * dsn_psi<R>(D.ph[1][2][1], T.bh[2][1][qz_hi - 1], T.ch[2][1][qz_hi - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hzv = hzv + DB * dsn_psi<R>(D.ph[2][0][0], T.bh[0][0][qx_lo - 1], T.ch[0][0][qx_lo - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hzv = hzv + DB * dsn_psi<R>(D.ph[2][0][1], T.bh[0][1][qx_hi - 1], T.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qy_lo) hzv = hzv + DB * dsn_psi<R>(D.ph[2][1][0], T.bh[1][0][qy_lo - 1], T.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hzv = hzv + DB * dsn_psi<R>(D.ph[2][1][1], T.bh[1][1][qy_hi - 1], T.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+        }
         Hx[c] = hxv;
         Hy[c] = hyv;
         Hz[c] = hzv;
+        ex = ex_kp;
+        ey = ey_kp;
     }
 }
 
+// E update of one component: bulk, then the CPML psi terms of its two
+// difference axes (ax1 with d1, ax2 with d2), as k_update_e
 template <typename R>
-__global__ void __launch_bounds__(256) k_dsn_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int slot) {
+__device__ __forceinline__ R dsn_e1(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, R eold, R d1, R d2, float den1,
+                                    float den2, R ga, R gb, bool pml, int q1l, int q1h, int q2l, int q2h, int px, int py,
+                                    int pz) {
+    const R curl = d1 * den1 + d2 * den2;
+    R e = ga * eold + gb * curl;
+    if (pml) {
+        const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
+        if (q1l) e = e + gb * dsn_psi<R>(D.pe[comp][ax1][0], T.be[ax1][0][q1l - 1], T.ce[ax1][0][q1l - 1], d1, P.del[ax1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
+        if (q1h) e = e + gb * dsn_psi<R>(D.pe[comp][ax1][1], T.be[ax1][1][q1h - 1], T.ce[ax1][1][q1h - 1], d1, P.del[ax1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
+        if (q2l) e = e + gb * dsn_psi<R>(D.pe[comp][ax2][0], T.be[ax2][0][q2l - 1], T.ce[ax2][0][q2l - 1], d2, P.del[ax2], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
+        if (q2h) e = e + gb * dsn_psi<R>(D.pe[comp][ax2][1], T.be[ax2][1][q2h - 1], T.ce[ax2][1][q2h - 1], d2, P.del[ax2], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
+    }
+    return e;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, 5) k_dsn_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int slot) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
+    __shared__ DsnTabs T;
+    load_tabs(P, T);
     if (px > P.SX - 2 || py > P.SY - 2) return;
     const R *Hx = D.H[0], *Hy = D.H[1], *Hz = D.H[2];
+    R *Ex = D.E[0], *Ey = D.E[1], *Ez = D.E[2];
     const int i = px + 1, j = py + 1;
     const float dex = P.den_e[0][i - 1], dey = P.den_e[1][j - 1];
     const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
     const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
+    const bool colpml = qxl || qxh || qyl || qyh;
+    const bool xok = px >= 1, yok = py >= 1, unavg_col = px == 0 || py == 0;
+    const bool coldsn = px >= D.lo[0] && px <= D.lo[0] + D.n[0] && py >= D.lo[1] && py <= D.lo[1] + D.n[1];
+    const uint8_t* C = P.cell;
     const long long PX = P.PX, PL = P.plane;
-    const int pz_end = min(P.SZ - 2, ((int)blockIdx.z + 1) * DZCH - 1);
-    for (int pz = blockIdx.z * DZCH; pz <= pz_end; pz++) {
+    const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
+    long long c = lin(P, px, py, pz0);
+    int b[4] = {0, 0, 0, 0};
+    R hx_m = 0, hy_m = 0;  // Hx, Hy of the plane below
+    if (pz0 > 0) {
+        const long long cm = c - PL;
+        if (!unavg_col) { b[0] = ldg_id(C + cm); b[1] = ldg_id(C + cm - 1); b[2] = ldg_id(C + cm - PX); b[3] = ldg_id(C + cm - 1 - PX); }
+        hx_m = ldg(Hx + cm);
+        hy_m = ldg(Hy + cm);
+    }
+    for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
         const int k = pz + 1;
-        const long long c = lin(P, px, py, pz);
+        int a[4] = {0, 0, 0, 0};
+        if (!unavg_col) { a[0] = ldg_id(C + c); a[1] = ldg_id(C + c - 1); a[2] = ldg_id(C + c - PX); a[3] = ldg_id(C + c - 1 - PX); }
         const float dez = P.den_e[2][k - 1];
         const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
-        const R hx = Hx[c], hy = Hy[c], hz = Hz[c];
-        for (int comp = 0; comp < 3; comp++) {
-            if (!e_upd(P, comp, px, py, pz)) continue;
-            R d1, d2;
-            float den1, den2;
-            if (comp == 0) { d1 = hz - Hz[c - PX]; den1 = dey; d2 = Hy[c - PL] - hy; den2 = dez; }
-            else if (comp == 1) { d1 = Hz[c - 1] - hz; den1 = dex; d2 = hx - Hx[c - PL]; den2 = dez; }
-            else { d1 = hy - Hy[c - 1]; den1 = dex; d2 = Hx[c - PX] - hx; den2 = dey; }
-            const R curl = d1 * den1 + d2 * den2;
-            R ga, gb;
-            dsn_coef(P, D, comp, px, py, pz, ga, gb);
-            R* Ec = D.E[comp];
-            R e = ga * Ec[c] + gb * curl;
-            const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
-            const int q1l = ax1 == 0 ? qxl : qyl, q1h = ax1 == 0 ? qxh : qyh;
-            const int q2l = ax2 == 1 ? qyl : qzl, q2h = ax2 == 1 ? qyh : qzh;
-            if (q1l) e = e + gb * dsn_psi<R>(D.pe[comp][ax1][0], P.be[ax1][0][q1l - 1], P.ce[ax1][0][q1l - 1], d1, P.del[ax1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
-            if (q1h) e = e + gb * dsn_psi<R>(D.pe[comp][ax1][1], P.be[ax1][1][q1h - 1], P.ce[ax1][1][q1h - 1], d1, P.del[ax1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
-            if (q2l) e = e + gb * dsn_psi<R>(D.pe[comp][ax2][0], P.be[ax2][0][q2l - 1], P.ce[ax2][0][q2l - 1], d2, P.del[ax2], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
-            if (q2h) e = e + gb * dsn_psi<R>(D.pe[comp][ax2][1], P.be[ax2][1][q2h - 1], P.ce[ax2][1][q2h - 1], d2, P.del[ax2], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
-            Ec[c] = e;
-            long long q;
-            if (slot >= 0 && dsn_edge(D, comp, px, py, pz, &q)) D.rec[slot * D.nedge + q] = e;
+        const bool pml = colpml || qzl || qzh;
+        const R hx = ldg(Hx + c), hy = ldg(Hy + c), hz = ldg(Hz + c);
+        R ga[3], gb[3];
+        coef3(P, T, unavg_col || pz == 0, a, b, ga, gb);
+        const bool dsn = coldsn && pz >= D.lo[2] && pz <= D.lo[2] + D.n[2];
+        long long q[3] = {-1, -1, -1};
+        if (dsn)
+            for (int cc = 0; cc < 3; cc++)
+                if (dsn_edge(D, cc, px, py, pz, &q[cc])) { ga[cc] = D.ga[q[cc]]; gb[cc] = D.gb[q[cc]]; }
+                else q[cc] = -1;
+        if (yok && pz >= 1) {
+            const R e = dsn_e1(P, T, D, 0, ldg(Ex + c), hz - ldg(Hz + c - PX), hy_m - hy, dey, dez, ga[0], gb[0], pml, qyl, qyh, qzl, qzh, px, py, pz);
+            Ex[c] = e;
+            if (slot >= 0 && q[0] >= 0) D.rec[slot * D.nedge + q[0]] = e;
         }
+        if (xok && pz >= 1) {
+            const R e = dsn_e1(P, T, D, 1, ldg(Ey + c), ldg(Hz + c - 1) - hz, hx - hx_m, dex, dez, ga[1], gb[1], pml, qxl, qxh, qzl, qzh, px, py, pz);
+            Ey[c] = e;
+            if (slot >= 0 && q[1] >= 0) D.rec[slot * D.nedge + q[1]] = e;
+        }
+        if (xok && yok) {
+            const R e = dsn_e1(P, T, D, 2, ldg(Ez + c), hy - ldg(Hy + c - 1), ldg(Hx + c - PX) - hx, dex, dey, ga[2], gb[2], pml, qxl, qxh, qyl, qyh, px, py, pz);
+            Ez[c] = e;
+            if (slot >= 0 && q[2] >= 0) D.rec[slot * D.nedge + q[2]] = e;
+        }
+        hx_m = hx;
+        hy_m = hy;
+        for (int t = 0; t < 4; t++) b[t] = a[t];
     }
 }
 
@@ -393,7 +501,7 @@ __global__ void k_adj_grad(const __grid_constant__ AemParams P, const __grid_con
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < D.nedge; q += (long long)gridDim.x * blockDim.x) {
         int px, py, pz;
         const int c = dsn_edge_pos(D, q, &px, &py, &pz);
-        const double lam = (double)D.lE[c][lin(P, px, py, pz)];
+        const double lam = (double)D.w[c][lin(P, px, py, pz)] / (double)D.gb[q];
         const double en = (double)D.rec[sn * D.nedge + q], em = (double)D.rec[sm * D.nedge + q];
         D.A[q] += lam * em;
         D.B[q] += lam * (en - (double)D.ga[q] * em);
@@ -412,9 +520,7 @@ __global__ void k_adj_ports_e(const __grid_constant__ AemParams P, const __grid_
         const double g = 2.0 * (D.dft[0] * co - D.dft[1] * s);
         R ga, gb;
         dsn_coef(P, D, D.pc, D.ppx, D.ppy, D.ppz, ga, gb);
-        const R l = D.lE[D.pc][D.pidx] + (R)g;
-        D.lE[D.pc][D.pidx] = l;
-        D.w[D.pc][D.pidx] = gb * l;
+        D.w[D.pc][D.pidx] = D.w[D.pc][D.pidx] + gb * (R)g;
         for (int n = 0; n < S.n; n++) {
             const PortDev& p = S.p[n];
             R sum = 0;
@@ -422,8 +528,9 @@ __global__ void k_adj_ports_e(const __grid_constant__ AemParams P, const __grid_
                 for (int b = p.loc[1]; b <= p.loc[1] + p.size[1] - 1; b++)
                     for (int c = p.loc[2]; c <= p.loc[2] + p.size[2] - 1; c++) {
                         const long long q = lin(P, a - 1, b - 1, c - 1);
-                        sum = sum + D.lE[p.dir][q];
-                        D.lE[p.dir][q] = 0;
+                        R pga, pgb;
+                        dsn_coef(P, D, p.dir, a - 1, b - 1, c - 1, pga, pgb);
+                        sum = sum + D.w[p.dir][q] / pgb;
                         D.w[p.dir][q] = 0;
                     }
             D.lV[n][1] = D.lV[n][1] + sum / (R)(p.sizef[p.dir] * p.dl[p.dir]);
@@ -495,119 +602,202 @@ __global__ void k_adj_ports_h(const __grid_constant__ AemParams P, const __grid_
     }
 }
 
-// adjoint of the difference term `which` (1: first axis, 2: second) of E
-// edge (comp) in the E update: den Gb lE plus the CPML psi adjoints of that
-// axis scaled by c/dl; 0 for an edge the bulk loop does not update
+// CPML part of the adjoint of E edge (comp)'s difference term along axis
+// `which` (1: first, 2: second difference axis): (c / dl) times the psi
+// adjoint of each E slab the edge lies in along that axis.  Edges the bulk
+// loop never updates hold zero adjoints, so no range test is needed.
 template <typename R>
-__device__ __forceinline__ R adj_d(const AemParams& P, const DsnDev<R>& D, int comp, int which, int px, int py, int pz) {
-    if (!e_upd(P, comp, px, py, pz)) return (R)0;
-    const long long c = lin(P, px, py, pz);
+__device__ __forceinline__ R pml_d(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, int which, int px, int py, int pz) {
     const int ax = which == 1 ? (comp == 0 ? 1 : 0) : (comp == 2 ? 1 : 2);
     const int r = (ax == 0 ? px : ax == 1 ? py : pz) + 1;
     const int N = ax == 0 ? P.X : ax == 1 ? P.Y : P.Z;
-    R v = P.den_e[ax][r - 1] * D.w[comp][c];
+    R v = 0;
     const int ql = (r >= 2 && r <= P.npml[ax][0]) ? r : 0, qh = (r >= N + 1 - P.npml[ax][1] && r <= N - 1) ? N + 1 - r : 0;
-    if (ql) v = v + dsn_div<R>(P.ce[ax][0][ql - 1] * D.se[comp][ax][0][psi_idx(P, ax, ql, px, py, pz, P.npml[ax][0])], P.del[ax]);
-    if (qh) v = v + dsn_div<R>(P.ce[ax][1][qh - 1] * D.se[comp][ax][1][psi_idx(P, ax, qh, px, py, pz, P.npml[ax][1])], P.del[ax]);
+    if (ql) v = v + dsn_div<R>(T.ce[ax][0][ql - 1] * D.se[comp][ax][0][psi_idx(P, ax, ql, px, py, pz, P.npml[ax][0])], P.del[ax]);
+    if (qh) v = v + dsn_div<R>(T.ce[ax][1][qh - 1] * D.se[comp][ax][1][psi_idx(P, ax, qh, px, py, pz, P.npml[ax][1])], P.del[ax]);
     return v;
 }
 
-// adjoint of the difference term along `ax` of H face (comp) in the H
-// update: DB den lH plus the CPML psi adjoints of that axis scaled by c/dl
+// CPML part of the adjoint of H face (comp)'s difference term along `ax`
 template <typename R>
-__device__ __forceinline__ R adj_m(const AemParams& P, const DsnDev<R>& D, int comp, int ax, int px, int py, int pz) {
-    if (!h_upd(P, px, py, pz)) return (R)0;
-    const long long c = lin(P, px, py, pz);
+__device__ __forceinline__ R pml_m(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, int ax, int px, int py, int pz) {
     const int r = (ax == 0 ? px : ax == 1 ? py : pz) + 1;
     const int N = ax == 0 ? P.X : ax == 1 ? P.Y : P.Z;
-    R v = (P.DB * P.den_h[ax][r - 1]) * D.lH[comp][c];
+    R v = 0;
     const int ql = (r <= P.npml[ax][0] - 1) ? r : 0, qh = (r >= N + 1 - P.npml[ax][1]) ? N - r : 0;
-    if (ql) v = v + dsn_div<R>(P.ch[ax][0][ql - 1] * D.sh[comp][ax][0][psi_idx(P, ax, ql, px, py, pz, P.npml[ax][0])], P.del[ax]);
-    if (qh) v = v + dsn_div<R>(P.ch[ax][1][qh - 1] * D.sh[comp][ax][1][psi_idx(P, ax, qh, px, py, pz, P.npml[ax][1])], P.del[ax]);
+    if (ql) v = v + dsn_div<R>(T.ch[ax][0][ql - 1] * D.sh[comp][ax][0][psi_idx(P, ax, ql, px, py, pz, P.npml[ax][0])], P.del[ax]);
+    if (qh) v = v + dsn_div<R>(T.ch[ax][1][qh - 1] * D.sh[comp][ax][1][psi_idx(P, ax, qh, px, py, pz, P.npml[ax][1])], P.del[ax]);
     return v;
 }
 
-// E half-step transposed, per H face: lH += (E update)^T [Gb lE, se]; then
-// sh = b sh + DB lH on CPML faces
+__device__ __forceinline__ bool e_slab(const AemParams& P, int ax, int r) {
+    const int N = ax == 0 ? P.X : ax == 1 ? P.Y : P.Z;
+    return (r >= 2 && r <= P.npml[ax][0]) || (r >= N + 1 - P.npml[ax][1] && r <= N - 1);
+}
+__device__ __forceinline__ bool h_slab(const AemParams& P, int ax, int r) {
+    const int N = ax == 0 ? P.X : ax == 1 ? P.Y : P.Z;
+    return r >= 1 && ((r <= P.npml[ax][0] - 1) || (r >= N + 1 - P.npml[ax][1] && r <= N - 1));
+}
+
+// E half-step transposed, per H face: lH += (E update)^T [w = Gb lE, se];
+// then sh = b sh + DB lH on CPML faces.  E update of edge e:
+// E_e = Ga E_e + Gb (d1 den1 + d2 den2) (+ Gb psi), so the adjoint of its
+// difference d is den w_e (+ c/dl se), scattered to the two faces of d.
 template <typename R>
-__global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
+__global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
+    __shared__ DsnTabs T;
+    load_tabs(P, T);
     if (px > P.SX - 2 || py > P.SY - 2) return;
+    const R *wX = D.w[0], *wY = D.w[1], *wZ = D.w[2];
+    R *lHx = D.lH[0], *lHy = D.lH[1], *lHz = D.lH[2];
     const int i = px + 1, j = py + 1;
     const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
     const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+    const bool colph = qx_lo || qx_hi || qy_lo || qy_hi;
+    // neighbouring E edges in a CPML slab along x / y (this face's edges at
+    // px, px+1 and py, py+1)
+    const bool pex = e_slab(P, 0, px + 1) || e_slab(P, 0, px + 2), pey = e_slab(P, 1, py + 1) || e_slab(P, 1, py + 2);
+    const float dex0 = P.den_e[0][px], dex1 = P.den_e[0][px + 1], dey0 = P.den_e[1][py], dey1 = P.den_e[1][py + 1];
     const float DB = P.DB;
-    const int pz_end = min(P.SZ - 2, ((int)blockIdx.z + 1) * DZCH - 1);
-    for (int pz = blockIdx.z * DZCH; pz <= pz_end; pz++) {
+    const long long PX = P.PX, PL = P.plane;
+    const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
+    long long c = lin(P, px, py, pz0);
+    R wx0 = ldg(wX + c), wy0 = ldg(wY + c);
+    for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
         const int k = pz + 1;
-        const long long c = lin(P, px, py, pz);
+        const float dez0 = P.den_e[2][pz], dez1 = P.den_e[2][pz + 1];
+        const R wxk = ldg(wX + c + PL), wyk = ldg(wY + c + PL), wz0 = ldg(wZ + c);
+        const R wxj = ldg(wX + c + PX), wyi = ldg(wY + c + 1), wzi = ldg(wZ + c + 1), wzj = ldg(wZ + c + PX);
+        R lx = ldg(lHx + c) + ((dez0 * wy0 - dez1 * wyk) - (dey0 * wz0 - dey1 * wzj));
+        R ly = ldg(lHy + c) + ((dez1 * wxk - dez0 * wx0) + (dex0 * wz0 - dex1 * wzi));
+        R lz = ldg(lHz + c) + ((dey0 * wx0 - dey1 * wxj) - (dex0 * wy0 - dex1 * wyi));
+        if (e_slab(P, 2, pz + 1) || e_slab(P, 2, pz + 2)) {  // z differences: Ey (Hx), Ex (Hy)
+            lx = lx + (pml_d(P, T, D, 1, 2, px, py, pz) - pml_d(P, T, D, 1, 2, px, py, pz + 1));
+            ly = ly + (pml_d(P, T, D, 0, 2, px, py, pz + 1) - pml_d(P, T, D, 0, 2, px, py, pz));
+        }
+        if (pey) {  // y differences: Ez (Hx), Ex (Hz)
+            lx = lx - (pml_d(P, T, D, 2, 2, px, py, pz) - pml_d(P, T, D, 2, 2, px, py + 1, pz));
+            lz = lz + (pml_d(P, T, D, 0, 1, px, py, pz) - pml_d(P, T, D, 0, 1, px, py + 1, pz));
+        }
+        if (pex) {  // x differences: Ez (Hy), Ey (Hz)
+            ly = ly + (pml_d(P, T, D, 2, 1, px, py, pz) - pml_d(P, T, D, 2, 1, px + 1, py, pz));
+            lz = lz - (pml_d(P, T, D, 1, 1, px, py, pz) - pml_d(P, T, D, 1, 1, px + 1, py, pz));
+        }
+        lHx[c] = lx;
+        lHy[c] = ly;
+        lHz[c] = lz;
         const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-        const R lx = D.lH[0][c] + (adj_d(P, D, 1, 2, px, py, pz) - adj_d(P, D, 1, 2, px, py, pz + 1) -
-                                   adj_d(P, D, 2, 2, px, py, pz) + adj_d(P, D, 2, 2, px, py + 1, pz));
-        const R ly = D.lH[1][c] + (adj_d(P, D, 0, 2, px, py, pz + 1) - adj_d(P, D, 0, 2, px, py, pz) +
-                                   adj_d(P, D, 2, 1, px, py, pz) - adj_d(P, D, 2, 1, px + 1, py, pz));
-        const R lz = D.lH[2][c] + (adj_d(P, D, 0, 1, px, py, pz) - adj_d(P, D, 0, 1, px, py + 1, pz) -
-                                   adj_d(P, D, 1, 1, px, py, pz) + adj_d(P, D, 1, 1, px + 1, py, pz));
-        D.lH[0][c] = lx;
-        D.lH[1][c] = ly;
-        D.lH[2][c] = lz;
-        auto upd = [&](R* s, float b, long long q, R l) { s[q] = b * s[q] + DB * l; };
-        if (qy_lo) upd(D.sh[0][1][0], P.bh[1][0][qy_lo - 1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]), lx);
-        if (qy_hi) upd(D.sh[0][1][1], P.bh[1][1][qy_hi - 1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]), lx);
-        if (qz_lo) upd(D.sh[0][2][0], P.bh[2][0][qz_lo - 1], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]), lx);
-        if (qz_hi) upd(D.sh[0][2][1], P.bh[2][1][qz_hi - 1], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]), lx);
-        if (qx_lo) upd(D.sh[1][0][0], P.bh[0][0][qx_lo - 1], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]), ly);
-        if (qx_hi) upd(D.sh[1][0][1], P.bh[0][1][qx_hi - 1], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]), ly);
-        if (qz_lo) upd(D.sh[1][2][0], P.bh[2][0][qz_lo - 1], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]), ly);
-        if (qz_hi) upd(D.sh[1][2][1], P.bh[2][1][qz_hi - 1], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]), ly);
-        if (qx_lo) upd(D.sh[2][0][0], P.bh[0][0][qx_lo - 1], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]), lz);
-        if (qx_hi) upd(D.sh[2][0][1], P.bh[0][1][qx_hi - 1], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]), lz);
-        if (qy_lo) upd(D.sh[2][1][0], P.bh[1][0][qy_lo - 1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]), lz);
-        if (qy_hi) upd(D.sh[2][1][1], P.bh[1][1][qy_hi - 1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]), lz);
+        if (colph || qz_lo || qz_hi) {
+            auto upd = [&](R* s, float b, long long q, R l) { s[q] = b * s[q] + DB * l; };
+            if (qy_lo) upd(D.sh[0][1][0], T.bh[1][0][qy_lo - 1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]), lx);
+            if (qy_hi) upd(D.sh[0][1][1], T.bh[1][1][qy_hi - 1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]), lx);
+            if (qz_lo) upd(D.sh[0][2][0], T.bh[2][0][qz_lo - 1], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]), lx);
+            if (qz_hi) upd(D.sh[0][2][1], T.bh[2][1][qz_hi - 1], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]), lx);
+            if (qx_lo) upd(D.sh[1][0][0], T.bh[0][0][qx_lo - 1], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]), ly);
+            if (qx_hi) upd(D.sh[1][0][1], T.bh[0][1][qx_hi - 1], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]), ly);
+            if (qz_lo) upd(D.sh[1][2][0], T.bh[2][0][qz_lo - 1], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]), ly);
+            if (qz_hi) upd(D.sh[1][2][1], T.bh[2][1][qz_hi - 1], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]), ly);
+            if (qx_lo) upd(D.sh[2][0][0], T.bh[0][0][qx_lo - 1], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]), lz);
+            if (qx_hi) upd(D.sh[2][0][1], T.bh[0][1][qx_hi - 1], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]), lz);
+            if (qy_lo) upd(D.sh[2][1][0], T.bh[1][0][qy_lo - 1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]), lz);
+            if (qy_hi) upd(D.sh[2][1][1], T.bh[1][1][qy_hi - 1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]), lz);
+        }
+        wx0 = wxk;
+        wy0 = wyk;
     }
 }
 
-// H half-step transposed, per E edge: lE = Ga lE + (H update)^T [lH, sh];
-// w = Gb lE; se = b se + w on CPML edges
+// Adjoint of one E edge through the H half-step.  The adjoint state kept
+// per edge is w = Gb lE (Gb > 0 for every material), so lE = Ga lE + g
+// becomes w = Ga w + Gb g; then se = b se + w on its CPML slabs
 template <typename R>
-__global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
+__device__ __forceinline__ void adj_e1(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, long long c, R g, R ga, R gb,
+                                       bool pml, int q1l, int q1h, int q2l, int q2h, int px, int py, int pz) {
+    const R wv = ga * ldg(D.w[comp] + c) + gb * g;
+    D.w[comp][c] = wv;
+    if (pml) {
+        const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
+        auto upd = [&](R* s, float b, long long q) { s[q] = b * s[q] + wv; };
+        if (q1l) upd(D.se[comp][ax1][0], T.be[ax1][0][q1l - 1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
+        if (q1h) upd(D.se[comp][ax1][1], T.be[ax1][1][q1h - 1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
+        if (q2l) upd(D.se[comp][ax2][0], T.be[ax2][0][q2l - 1], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
+        if (q2h) upd(D.se[comp][ax2][1], T.be[ax2][1][q2h - 1], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
+    }
+}
+
+// H half-step transposed, per E edge: the H update
+// H_f += DB (d1 den1 + d2 den2) (+ DB psi) gives each of the face's two
+// differences the adjoint DB den lH_f (+ c/dl sh), gathered here from the
+// four faces around the edge
+template <typename R>
+__global__ void __launch_bounds__(256, 5) k_adj_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
+    __shared__ DsnTabs T;
+    load_tabs(P, T);
     if (px > P.SX - 2 || py > P.SY - 2) return;
+    const R *lHx = D.lH[0], *lHy = D.lH[1], *lHz = D.lH[2];
     const int i = px + 1, j = py + 1;
     const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
     const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
-    const int pz_end = min(P.SZ - 2, ((int)blockIdx.z + 1) * DZCH - 1);
-    for (int pz = blockIdx.z * DZCH; pz <= pz_end; pz++) {
+    const bool colpe = qxl || qxh || qyl || qyh;
+    // neighbouring H faces in a CPML slab along x / y (faces at px-1, px and
+    // py-1, py)
+    const bool phx = h_slab(P, 0, px + 1) || h_slab(P, 0, px), phy = h_slab(P, 1, py + 1) || h_slab(P, 1, py);
+    const bool xok = px >= 1, yok = py >= 1, unavg_col = px == 0 || py == 0;
+    const bool coldsn = px >= D.lo[0] && px <= D.lo[0] + D.n[0] && py >= D.lo[1] && py <= D.lo[1] + D.n[1];
+    const float DB = P.DB;
+    const float bx0 = DB * P.den_h[0][px], bxm = xok ? DB * P.den_h[0][px - 1] : 0.0f;
+    const float by0 = DB * P.den_h[1][py], bym = yok ? DB * P.den_h[1][py - 1] : 0.0f;
+    const uint8_t* C = P.cell;
+    const long long PX = P.PX, PL = P.plane;
+    const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
+    long long c = lin(P, px, py, pz0);
+    int b[4] = {0, 0, 0, 0};
+    R lx_m = 0, ly_m = 0;  // lHx, lHy of the plane below
+    if (pz0 > 0) {
+        const long long cm = c - PL;
+        if (!unavg_col) { b[0] = ldg_id(C + cm); b[1] = ldg_id(C + cm - 1); b[2] = ldg_id(C + cm - PX); b[3] = ldg_id(C + cm - 1 - PX); }
+        lx_m = ldg(lHx + cm);
+        ly_m = ldg(lHy + cm);
+    }
+    for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
         const int k = pz + 1;
-        const long long c = lin(P, px, py, pz);
+        int a[4] = {0, 0, 0, 0};
+        if (!unavg_col) { a[0] = ldg_id(C + c); a[1] = ldg_id(C + c - 1); a[2] = ldg_id(C + c - PX); a[3] = ldg_id(C + c - 1 - PX); }
+        const float bz0 = DB * P.den_h[2][pz], bzm = pz >= 1 ? DB * P.den_h[2][pz - 1] : 0.0f;
         const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
-        for (int comp = 0; comp < 3; comp++) {
-            if (!e_upd(P, comp, px, py, pz)) continue;
-            R g;
-            if (comp == 0)
-                g = adj_m(P, D, 1, 2, px, py, pz) - adj_m(P, D, 1, 2, px, py, pz - 1) + adj_m(P, D, 2, 1, px, py - 1, pz) -
-                    adj_m(P, D, 2, 1, px, py, pz);
-            else if (comp == 1)
-                g = adj_m(P, D, 0, 2, px, py, pz - 1) - adj_m(P, D, 0, 2, px, py, pz) + adj_m(P, D, 2, 0, px, py, pz) -
-                    adj_m(P, D, 2, 0, px - 1, py, pz);
-            else
-                g = adj_m(P, D, 0, 1, px, py, pz) - adj_m(P, D, 0, 1, px, py - 1, pz) + adj_m(P, D, 1, 0, px - 1, py, pz) -
-                    adj_m(P, D, 1, 0, px, py, pz);
-            R ga, gb;
-            dsn_coef(P, D, comp, px, py, pz, ga, gb);
-            const R l = ga * D.lE[comp][c] + g;
-            const R wv = gb * l;
-            D.lE[comp][c] = l;
-            D.w[comp][c] = wv;
-            const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
-            const int q1l = ax1 == 0 ? qxl : qyl, q1h = ax1 == 0 ? qxh : qyh;
-            const int q2l = ax2 == 1 ? qyl : qzl, q2h = ax2 == 1 ? qyh : qzh;
-            auto upd = [&](R* s, float b, long long q) { s[q] = b * s[q] + wv; };
-            if (q1l) upd(D.se[comp][ax1][0], P.be[ax1][0][q1l - 1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
-            if (q1h) upd(D.se[comp][ax1][1], P.be[ax1][1][q1h - 1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
-            if (q2l) upd(D.se[comp][ax2][0], P.be[ax2][0][q2l - 1], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
-            if (q2h) upd(D.se[comp][ax2][1], P.be[ax2][1][q2h - 1], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
+        const bool pe = colpe || qzl || qzh;
+        const bool phz = h_slab(P, 2, pz + 1) || h_slab(P, 2, pz);
+        const R lx = ldg(lHx + c), ly = ldg(lHy + c), lz = ldg(lHz + c);
+        R ga[3], gb[3];
+        coef3(P, T, unavg_col || pz == 0, a, b, ga, gb);
+        if (coldsn && pz >= D.lo[2] && pz <= D.lo[2] + D.n[2])
+            for (int cc = 0; cc < 3; cc++) {
+                long long q;
+                if (dsn_edge(D, cc, px, py, pz, &q)) { ga[cc] = D.ga[q]; gb[cc] = D.gb[q]; }
+            }
+        if (yok && pz >= 1) {  // Ex: d1 = Hz - Hz[j-1] (y), d2 = Hy[k-1] - Hy (z)
+            R g = (bz0 * ly - bzm * ly_m) + (bym * ldg(lHz + c - PX) - by0 * lz);
+            if (phz) g = g + (pml_m(P, T, D, 1, 2, px, py, pz) - pml_m(P, T, D, 1, 2, px, py, pz - 1));
+            if (phy) g = g + (pml_m(P, T, D, 2, 1, px, py - 1, pz) - pml_m(P, T, D, 2, 1, px, py, pz));
+            adj_e1(P, T, D, 0, c, g, ga[0], gb[0], pe, qyl, qyh, qzl, qzh, px, py, pz);
         }
+        if (xok && pz >= 1) {  // Ey: d1 = Hz[i-1] - Hz (x), d2 = Hx - Hx[k-1] (z)
+            R g = (bzm * lx_m - bz0 * lx) + (bx0 * lz - bxm * ldg(lHz + c - 1));
+            if (phz) g = g + (pml_m(P, T, D, 0, 2, px, py, pz - 1) - pml_m(P, T, D, 0, 2, px, py, pz));
+            if (phx) g = g + (pml_m(P, T, D, 2, 0, px, py, pz) - pml_m(P, T, D, 2, 0, px - 1, py, pz));
+            adj_e1(P, T, D, 1, c, g, ga[1], gb[1], pe, qxl, qxh, qzl, qzh, px, py, pz);
+        }
+        if (xok && yok) {  // Ez: d1 = Hy - Hy[i-1] (x), d2 = Hx[j-1] - Hx (y)
+            R g = (by0 * lx - bym * ldg(lHx + c - PX)) + (bxm * ldg(lHy + c - 1) - bx0 * ly);
+            if (phy) g = g + (pml_m(P, T, D, 0, 1, px, py, pz) - pml_m(P, T, D, 0, 1, px, py - 1, pz));
+            if (phx) g = g + (pml_m(P, T, D, 1, 0, px - 1, py, pz) - pml_m(P, T, D, 1, 0, px, py, pz));
+            adj_e1(P, T, D, 2, c, g, ga[2], gb[2], pe, qxl, qxh, qyl, qyh, px, py, pz);
+        }
+        lx_m = lx;
+        ly_m = ly;
+        for (int t = 0; t < 4; t++) b[t] = a[t];
     }
 }
 
@@ -678,8 +868,22 @@ class DsnImpl : public DesignRun {
         DSN_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st_));
         return (T*)p;
     }
-    void step(int n, int slot, int acc);
-    void adj_step(int n, int s0);
+    void step(int n, int slot, int acc, const DsnDev<R>& D, cudaStream_t st);
+    void adj_step(int n, int s0, const DsnDev<R>& D);
+    void recompute(int seg, const DsnDev<R>& D, cudaStream_t st);
+    DsnDev<R> with_rec(int seg) const {
+        DsnDev<R> d = D_;
+        d.rec = rec_[seg & 1];
+        return d;
+    }
+    cudaEvent_t seg_event(size_t q) {
+        while (seg_ev_.size() <= q) {
+            cudaEvent_t e;
+            DSN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            seg_ev_.push_back(e);
+        }
+        return seg_ev_[q];
+    }
     void zero(const std::vector<std::pair<void*, size_t>>& v) {
         for (auto& a : v) DSN_CUDA(cudaMemsetAsync(a.first, 0, a.second, st_));
     }
@@ -710,8 +914,13 @@ class DsnImpl : public DesignRun {
     int K_ = 0, nseg_ = 0;
     char* ck_ = nullptr;
     size_t ck_cap_ = 0;
-    R* rec_ = nullptr;
-    size_t rec_cap_ = 0;     // slots allocated
+    // design-box E records of one segment, two buffers: the adjoint sweep of
+    // one segment reads one while the next segment is recomputed into the
+    // other on the side stream
+    R* rec_[2] = {nullptr, nullptr};
+    size_t rec_cap_ = 0;     // slots allocated per buffer
+    cudaStream_t sb_ = nullptr;
+    std::vector<cudaEvent_t> seg_ev_;
     bool ready_ = false;     // forward() with checkpoints since set_design
     bool last_recorded_ = false;
     double* dft_ = nullptr;
@@ -768,12 +977,10 @@ DsnImpl<R>::DsnImpl(const std::string& inputs, const std::string& outdir, const 
     for (int c = 0; c < 3; c++) {
         D_.E[c] = alloc<R>(cells);
         D_.H[c] = alloc<R>(cells);
-        D_.lE[c] = alloc<R>(cells);
         D_.lH[c] = alloc<R>(cells);
         D_.w[c] = alloc<R>(cells);
         state_.push_back({D_.E[c], cells * sizeof(R)});
         state_.push_back({D_.H[c], cells * sizeof(R)});
-        adj_.push_back({D_.lE[c], cells * sizeof(R)});
         adj_.push_back({D_.lH[c], cells * sizeof(R)});
         adj_.push_back({D_.w[c], cells * sizeof(R)});
     }
@@ -816,6 +1023,7 @@ DsnImpl<R>::DsnImpl(const std::string& inputs, const std::string& outdir, const 
     D_.pc = -1;
     DSN_CUDA(cudaEventCreate(&ev_[0]));
     DSN_CUDA(cudaEventCreate(&ev_[1]));
+    DSN_CUDA(cudaStreamCreateWithFlags(&sb_, cudaStreamNonBlocking));
     DSN_CUDA(cudaStreamSynchronize(st_));
 }
 
@@ -824,9 +1032,13 @@ DsnImpl<R>::~DsnImpl() {
     if (st_) cudaStreamSynchronize(st_);
     for (void* p : bufs_) cudaFree(p);
     if (ck_) cudaFree(ck_);
-    if (rec_) cudaFree(rec_);
+    if (sb_) cudaStreamSynchronize(sb_);
+    for (R* r : rec_)
+        if (r) cudaFree(r);
     for (cudaEvent_t e : ev_)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : seg_ev_) cudaEventDestroy(e);
+    if (sb_) cudaStreamDestroy(sb_);
 }
 
 template <typename R>
@@ -890,27 +1102,46 @@ void DsnImpl<R>::set_design(const float* eps, const float* sig) {
 }
 
 template <typename R>
-void DsnImpl<R>::step(int n, int slot, int acc) {
-    D_.acc_dft = acc;
+void DsnImpl<R>::step(int n, int slot, int acc, const DsnDev<R>& Dv, cudaStream_t st) {
+    DsnDev<R> D = Dv;
+    D.acc_dft = acc;
     const dim3 blk(32, 8);
-    k_dsn_h<R><<<vgrid(), blk, 0, st_>>>(P_, D_);
-    k_dsn_ports_h<R><<<1, 256, 0, st_>>>(P_, S_, D_, n);
-    k_dsn_e<R><<<vgrid(), blk, 0, st_>>>(P_, D_, slot);
-    k_dsn_ports_e<R><<<1, 256, 0, st_>>>(P_, S_, D_, n);
+    k_dsn_h<R><<<vgrid(), blk, 0, st>>>(P_, D);
+    k_dsn_ports_h<R><<<1, 256, 0, st>>>(P_, S_, D, n);
+    k_dsn_e<R><<<vgrid(), blk, 0, st>>>(P_, D, slot);
+    k_dsn_ports_e<R><<<1, 256, 0, st>>>(P_, S_, D, n);
 }
 
 template <typename R>
-void DsnImpl<R>::adj_step(int n, int s0) {
+void DsnImpl<R>::adj_step(int n, int s0, const DsnDev<R>& D) {
     const dim3 blk(32, 8);
     if (n < steps_) {
-        k_adj_grad<R><<<egrid(D_.nedge), 256, 0, st_>>>(P_, D_, n - s0, n - 1 - s0);
+        k_adj_grad<R><<<egrid(D.nedge), 256, 0, st_>>>(P_, D, n - s0, n - 1 - s0);
         launches_[1]++;
     }
-    k_adj_ports_e<R><<<1, 256, 0, st_>>>(P_, S_, D_, n);
-    k_adj_h<R><<<vgrid(), blk, 0, st_>>>(P_, D_);
-    k_adj_ports_h<R><<<1, 256, 0, st_>>>(P_, S_, D_);
-    k_adj_e<R><<<vgrid(), blk, 0, st_>>>(P_, D_);
+    k_adj_ports_e<R><<<1, 256, 0, st_>>>(P_, S_, D, n);
+    k_adj_h<R><<<vgrid(), blk, 0, st_>>>(P_, D);
+    k_adj_ports_h<R><<<1, 256, 0, st_>>>(P_, S_, D);
+    k_adj_e<R><<<vgrid(), blk, 0, st_>>>(P_, D);
     launches_[1] += 4;
+}
+
+// forward steps of segment `seg` again from its checkpoint, recording the
+// design-box E history into D.rec
+template <typename R>
+void DsnImpl<R>::recompute(int seg, const DsnDev<R>& D, cudaStream_t st) {
+    const int s0 = seg * K_, s1 = std::min(s0 + K_, steps_);
+    const char* src = ck_ + (size_t)seg * state_bytes_;
+    for (auto& a : state_) {
+        DSN_CUDA(cudaMemcpyAsync(a.first, src, a.second, cudaMemcpyDeviceToDevice, st));
+        src += (a.second + 255) / 256 * 256;
+    }
+    k_dsn_record<R><<<egrid(D.nedge), 256, 0, st>>>(P_, D, 0);
+    launches_[1]++;
+    for (int n = s0 + 1; n <= s1; n++) {
+        step(n, n - s0, 0, D, st);
+        launches_[1] += 4;
+    }
 }
 
 template <typename R>
@@ -930,16 +1161,19 @@ double DsnImpl<R>::forward(int K, double dft[2]) {
             ck_cap_ = need_ck;
         }
         if ((size_t)(K + 1) > rec_cap_) {
-            if (rec_) cudaFree(rec_);
-            rec_ = nullptr;
+            for (R*& r : rec_) {
+                if (r) cudaFree(r);
+                r = nullptr;
+            }
             rec_cap_ = 0;
-            DSN_CUDA(cudaMalloc(&rec_, need_rec));
+            DSN_CUDA(cudaMalloc(&rec_[0], need_rec));
+            DSN_CUDA(cudaMalloc(&rec_[1], need_rec));
             rec_cap_ = K + 1;
         }
         K_ = K;
         nseg_ = nseg;
-        D_.rec = rec_;
     }
+    const DsnDev<R> D = plain ? D_ : with_rec(nseg_ - 1);
     zero(state_);
     DSN_CUDA(cudaMemsetAsync(dft_, 0, 2 * sizeof(double), st_));
     DSN_CUDA(cudaEventRecord(ev_[0], st_));
@@ -955,11 +1189,11 @@ double DsnImpl<R>::forward(int K, double dft[2]) {
             }
             if (s == nseg_ - 1) {
                 slot_base = n - 1;
-                k_dsn_record<R><<<egrid(D_.nedge), 256, 0, st_>>>(P_, D_, 0);
+                k_dsn_record<R><<<egrid(D.nedge), 256, 0, st_>>>(P_, D, 0);
                 launches_[0]++;
             }
         }
-        step(n, slot_base >= 0 ? n - slot_base : -1, 1);
+        step(n, slot_base >= 0 ? n - slot_base : -1, 1, D, st_);
         launches_[0] += 4;
     }
     DSN_CUDA(cudaEventRecord(ev_[1], st_));
@@ -976,32 +1210,47 @@ double DsnImpl<R>::forward(int K, double dft[2]) {
     return h[0] * h[0] + h[1] * h[1];
 }
 
+// The adjoint sweeps segments last to first on the run's stream.  Segment
+// s-1 is recomputed on the side stream while segment s is swept: the sweep
+// reads only its record buffer, the recompute writes the forward state and
+// the other buffer.  Events order each recompute after the sweep that last
+// read its buffer, and each sweep after its recompute.
 template <typename R>
 void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     if (!ready_) throw std::invalid_argument("design gradient: run forward() with checkpoints first");
-    const int N = steps_, K = K_;
+    const int N = steps_, K = K_, S = nseg_;
     zero(adj_);
     DSN_CUDA(cudaMemsetAsync(D_.A, 0, D_.nedge * sizeof(double), st_));
     DSN_CUDA(cudaMemsetAsync(D_.B, 0, D_.nedge * sizeof(double), st_));
     DSN_CUDA(cudaEventRecord(ev_[0], st_));
+    DSN_CUDA(cudaStreamWaitEvent(sb_, ev_[0], 0));
     launches_[1] = 0;
-    for (int s = nseg_ - 1; s >= 0; s--) {
+    auto ev_sweep = [&](int s) { return seg_event(2 * (size_t)s); };
+    auto ev_rec = [&](int s) { return seg_event(2 * (size_t)s + 1); };
+    auto sweep = [&](int s) {
+        const DsnDev<R> D = with_rec(s);
         const int s0 = s * K, s1 = std::min(s0 + K, N);
-        if (!(s == nseg_ - 1 && last_recorded_)) {
-            // recompute the segment from its checkpoint, recording E
-            const char* src = ck_ + (size_t)s * state_bytes_;
-            for (auto& a : state_) {
-                DSN_CUDA(cudaMemcpyAsync(a.first, src, a.second, cudaMemcpyDeviceToDevice, st_));
-                src += (a.second + 255) / 256 * 256;
-            }
-            k_dsn_record<R><<<egrid(D_.nedge), 256, 0, st_>>>(P_, D_, 0);
-            launches_[1]++;
-            for (int n = s0 + 1; n <= s1; n++) {
-                step(n, n - s0, 0);
-                launches_[1] += 4;
-            }
+        for (int n = s1; n > s0; n--) adj_step(n, s0, D);
+        DSN_CUDA(cudaEventRecord(ev_sweep(s), st_));
+    };
+    if (!last_recorded_) {
+        recompute(S - 1, with_rec(S - 1), st_);
+        DSN_CUDA(cudaEventRecord(ev_rec(S - 1), st_));
+        DSN_CUDA(cudaStreamWaitEvent(sb_, ev_rec(S - 1), 0));
+    }
+    if (S >= 2) {
+        recompute(S - 2, with_rec(S - 2), sb_);
+        DSN_CUDA(cudaEventRecord(ev_rec(S - 2), sb_));
+    }
+    sweep(S - 1);
+    for (int s = S - 2; s >= 0; s--) {
+        if (s >= 1) {
+            DSN_CUDA(cudaStreamWaitEvent(sb_, ev_sweep(s + 1), 0));
+            recompute(s - 1, with_rec(s - 1), sb_);
+            DSN_CUDA(cudaEventRecord(ev_rec(s - 1), sb_));
         }
-        for (int n = s1; n > s0; n--) adj_step(n, s0);
+        DSN_CUDA(cudaStreamWaitEvent(st_, ev_rec(s), 0));
+        sweep(s);
     }
     last_recorded_ = false;  // earlier segments' recomputes overwrote the records
     const long long ncell = (long long)D_.n[0] * D_.n[1] * D_.n[2];
@@ -1014,6 +1263,7 @@ void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     if (geps) DSN_CUDA(cudaMemcpyAsync(geps, out, ncell * sizeof(float), cudaMemcpyDefault, st_));
     if (gsig) DSN_CUDA(cudaMemcpyAsync(gsig, out + ncell, ncell * sizeof(float), cudaMemcpyDefault, st_));
     DSN_CUDA(cudaStreamSynchronize(st_));
+    DSN_CUDA(cudaStreamSynchronize(sb_));
     float t = 0;
     DSN_CUDA(cudaEventElapsedTime(&t, ev_[0], ev_[1]));
     ms_[1] = t;
