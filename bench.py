@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--adjoint-n", type=int, default=192, help="grid cells per axis of the design-gradient workload")
     ap.add_argument("--adjoint-steps", type=int, default=3000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=200, help="steps between forward checkpoints")
-    ap.add_argument("--adjoint-fd", type=int, default=0,
+    ap.add_argument("--adjoint-fd", type=int, default=2,
                     help="design cells checked against FP64 central differences (2 FP64 runs each)")
     return ap.parse_args()
 
@@ -286,6 +286,13 @@ def adjoint_gradient(args, max_over_ranks):
         dsn.forward(steps)
         g_all = dsn.gradient()
         t_fwd_all, t_grad_all, _, _ = dsn.timing()
+        sweep = {}
+        for k in (100, 50):
+            if k < steps and k != K:
+                dsn.forward(k)
+                dsn.gradient()
+                tf, tg, _, _ = dsn.timing()
+                sweep[str(k)] = round((max_over_ranks(tf) + max_over_ranks(tg)) / max_over_ranks(t_plain), 3)
         cells = n ** 3
         t_plain, t_fwd, t_grad = max_over_ranks(t_plain), max_over_ranks(t_fwd), max_over_ranks(t_grad)
         t_fwd_all, t_grad_all = max_over_ranks(t_fwd_all), max_over_ranks(t_grad_all)
@@ -295,6 +302,7 @@ def adjoint_gradient(args, max_over_ranks):
                     "ratio": round((t_fwd + t_grad) / t_plain, 3),
                     "store_all_forward_ms": round(t_fwd_all, 2), "store_all_gradient_ms": round(t_grad_all, 2),
                     "store_all_ratio": round((t_fwd_all + t_grad_all) / t_plain, 3),
+                    "ratio_by_checkpoint_interval": sweep,
                     "gradient_launches": l_grad, "forward_launches": l_fwd,
                     "segments_equal": bool(np.array_equal(g, g_all)), "fom_equal": f_plain == f_ck,
                     "grad_abs_max": float(np.abs(g).max())})
