@@ -76,6 +76,8 @@ def load_library():
     lib.aem_dft.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
                             ctypes.c_void_p, ctypes.c_void_p]
     lib.aem_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]
+    lib.aem_dft_batch.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_longlong, ctypes.c_double,
+                                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     lib.aem_transfer_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     i3 = ctypes.c_int * 3
     lib.aem_design_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i3, i3, ctypes.c_int, ctypes.POINTER(h)]
@@ -112,6 +114,25 @@ def dft(x, dt, freqs, stream=0):
     if rc != 0:
         raise AemError(lib.aem_last_error(None).decode())
     return torch.view_as_complex(out.view(-1, 2))
+
+
+def dft_batch(x, dt, freqs, stream=0):
+    """Spectra of the rows of `x` (CUDA float64, shape (nseries, n)) at
+    `freqs` (CUDA float64, Hz): sum_m x[s, m] exp(-i 2 pi f m dt), as a
+    complex128 CUDA tensor (nseries, nf).  Runs aem_dft_batch on `stream`
+    (default: the current stream)."""
+    import torch
+    lib = load_library()
+    if x.dtype != torch.float64 or not x.is_cuda or x.dim() != 2 or freqs.dtype != torch.float64 or not freqs.is_cuda:
+        raise ValueError("x must be a 2-D CUDA float64 tensor and freqs a CUDA float64 tensor")
+    x, freqs = x.contiguous(), freqs.contiguous()
+    ns, n = x.shape
+    out = torch.empty((ns, 2 * freqs.numel()), dtype=torch.float64, device=x.device)
+    st = stream or torch.cuda.current_stream(x.device).cuda_stream
+    rc = lib.aem_dft_batch(x.data_ptr(), n, ns, n, float(dt), freqs.data_ptr(), freqs.numel(), out.data_ptr(), st)
+    if rc != 0:
+        raise AemError(lib.aem_last_error(None).decode())
+    return torch.view_as_complex(out.view(ns, -1, 2))
 
 
 def check_deck(deck_text, ext_text=None, kmax=False):

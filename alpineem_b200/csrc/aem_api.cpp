@@ -299,6 +299,28 @@ int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf,
     return AEM_OK;
 }
 
+int aem_dft_batch(const double* x, long long ld, int nseries, long long n, double dt, const double* freqs, int nf,
+                  double* out, void* stream) {
+    if (!x || !freqs || !out || n < 1 || nf < 1 || nseries < 1 || ld < n || !(dt > 0.0))
+        return fail(nullptr, AEM_ERR_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int chunks = aem::dftb_chunks(n, nseries, nf);
+    double* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&scratch, sizeof(double) * 2 * (size_t)chunks * nseries * nf, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, AEM_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    }
+    e = aem::dftb_launch(x, ld, nseries, n, dt, freqs, nf, out, scratch, chunks, s);
+    cudaError_t e2 = cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, AEM_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    }
+    return AEM_OK;
+}
+
 int aem_grid(aem_handle* h, int sizes[3]) {
     if (!h || !sizes) return AEM_ERR_ARG;
     const aem::Deck& d = h->s->deck();

@@ -70,3 +70,97 @@ cudaError_t dft_launch(const float* x, long long n, double dt, const double* fre
 }
 
 }  // namespace aem
+
+// ---------------------------------------------------------------------------
+// Batched spectra of many series sampled alike (every far-field angle and
+// polarisation, the ports, the incident wave of a run):
+//   X[s][f] = sum_{m=0}^{n-1} x[s*ld + m] exp(-i 2 pi f m dt).
+// Thread f of a CTA holds DFTB_SERIES accumulators; the samples of those
+// series arrive in shared-memory tiles read by every thread, so the twiddle
+// of (f, m) is computed once for DFTB_SERIES series.  The sample range may
+// be cut into chunks (grid y) summed afterwards in chunk order, so results
+// do not depend on scheduling.
+namespace aem {
+namespace {
+constexpr int DFTB_SERIES = 8, DFTB_TILE = 256, DFTB_T = 128;
+
+__global__ void __launch_bounds__(DFTB_T) k_dftb_partial(const double* __restrict__ x, long long ld, int ns, long long n,
+                                                         double dt, const double* __restrict__ freqs, int nf, int chunks,
+                                                         double* __restrict__ part) {
+    __shared__ double tile[DFTB_SERIES][DFTB_TILE];
+    const int f = blockIdx.x * DFTB_T + threadIdx.x;
+    const int s0 = blockIdx.z * DFTB_SERIES;
+    const int chunk = blockIdx.y;
+    const long long len = (n + chunks - 1) / chunks;
+    const long long m0 = (long long)chunk * len, m1 = m0 + len < n ? m0 + len : n;
+    const double a = f < nf ? 2.0 * freqs[f] * dt : 0.0;  // half-turns per sample
+    double re[DFTB_SERIES], im[DFTB_SERIES];
+    for (int q = 0; q < DFTB_SERIES; q++) re[q] = im[q] = 0.0;
+    for (long long t0 = m0; t0 < m1; t0 += DFTB_TILE) {
+        const int tl = (int)(m1 - t0 < DFTB_TILE ? m1 - t0 : DFTB_TILE);
+        __syncthreads();
+        for (int e = threadIdx.x; e < DFTB_SERIES * DFTB_TILE; e += DFTB_T) {
+            const int q = e / DFTB_TILE, m = e % DFTB_TILE;
+            tile[q][m] = (s0 + q < ns && m < tl) ? x[(long long)(s0 + q) * ld + t0 + m] : 0.0;
+        }
+        __syncthreads();
+        if (f < nf)
+            for (int m = 0; m < tl; m++) {
+                double ph = a * (double)(t0 + m);
+                ph -= 2.0 * floor(0.5 * ph);
+                double sn, cs;
+                sincospi(ph, &sn, &cs);
+#pragma unroll
+                for (int q = 0; q < DFTB_SERIES; q++) {
+                    const double v = tile[q][m];
+                    re[q] += v * cs;
+                    im[q] -= v * sn;
+                }
+            }
+    }
+    if (f >= nf) return;
+    for (int q = 0; q < DFTB_SERIES; q++) {
+        if (s0 + q >= ns) break;
+        const long long o = 2 * (((long long)chunk * ns + s0 + q) * nf + f);
+        part[o] = re[q];
+        part[o + 1] = im[q];
+    }
+}
+
+__global__ void k_dftb_reduce(const double* __restrict__ part, int ns, int nf, int chunks, double* __restrict__ out) {
+    const long long tot = (long long)ns * nf;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int c = 0; c < chunks; c++) {
+            re += part[2 * ((long long)c * tot + e)];
+            im += part[2 * ((long long)c * tot + e) + 1];
+        }
+        out[2 * e] = re;
+        out[2 * e + 1] = im;
+    }
+}
+}  // namespace
+
+int dftb_chunks(long long n, int ns, int nf) {
+    // enough CTAs for every SM several times over, each chunk at least
+    // DFTB_TILE samples
+    const long long ctas = (long long)((nf + DFTB_T - 1) / DFTB_T) * ((ns + DFTB_SERIES - 1) / DFTB_SERIES);
+    long long c = (148LL * 8 + ctas - 1) / ctas;
+    const long long cmax = (n + DFTB_TILE - 1) / DFTB_TILE;
+    if (c > cmax) c = cmax;
+    if (c > 64) c = 64;
+    return c < 1 ? 1 : (int)c;
+}
+
+cudaError_t dftb_launch(const double* x, long long ld, int ns, long long n, double dt, const double* freqs, int nf,
+                        double* out, double* scratch, int chunks, cudaStream_t s) {
+    dim3 g((nf + DFTB_T - 1) / DFTB_T, chunks, (ns + DFTB_SERIES - 1) / DFTB_SERIES);
+    if (g.z > 65535) return cudaErrorInvalidValue;
+    k_dftb_partial<<<g, DFTB_T, 0, s>>>(x, ld, ns, n, dt, freqs, nf, chunks, scratch);
+    const long long tot = (long long)ns * nf;
+    const int blocks = (int)((tot + 255) / 256 < 148 * 16 ? (tot + 255) / 256 : 148 * 16);
+    k_dftb_reduce<<<blocks, 256, 0, s>>>(scratch, ns, nf, chunks, out);
+    return cudaGetLastError();
+}
+
+}  // namespace aem

@@ -15,4 +15,10 @@ int dft_chunks(long long n, int nf);
 cudaError_t dft_launch(const float* x, long long n, double dt, const double* freqs, int nf, double* out,
                        double* scratch, int chunks, cudaStream_t s);
 
+// batched spectra of ns series (row stride ld, FP64 samples); `scratch`
+// holds 2 * chunks * ns * nf doubles, out 2 * ns * nf (series-major)
+int dftb_chunks(long long n, int ns, int nf);
+cudaError_t dftb_launch(const double* x, long long ld, int ns, long long n, double dt, const double* freqs, int nf,
+                        double* out, double* scratch, int chunks, cudaStream_t s);
+
 }  // namespace aem

@@ -153,6 +153,16 @@ int aem_far_field_size(aem_handle* h, long long* face_cells, int* angles);
  * of 16 * chunks * nf bytes (chunks <= 64) from the stream-ordered pool. */
 int aem_dft(const float* x, long long n, double dt, const double* freqs, int nf, double* out, void* stream);
 
+/* Spectra of nseries series at once (every far-field angle and port of a
+ * run): out[2*(s*nf + k)] + i out[2*(s*nf + k) + 1] =
+ * sum_{m<n} x[s*ld + m] exp(-i 2 pi freqs[k] m dt).  FP64 samples (the
+ * post-processor reads the .dat text as float64), FP64 accumulation;
+ * device pointers, deterministic.  The spectra of post_processor.py
+ * (:160-215, numpy's FFT of the zero-padded series, kept in the trusted
+ * band :299-307) are these sums at the band's FFT bins. */
+int aem_dft_batch(const double* x, long long ld, int nseries, long long n, double dt, const double* freqs, int nf,
+                  double* out, void* stream);
+
 /* aem_dft for callers that cannot allocate device memory (an application
  * that keeps all GPU memory in its own arena, a plugin host that forbids
  * allocation in its callbacks, a real-time loop that must not block on an
