@@ -271,7 +271,7 @@ __device__ __forceinline__ void coef3(const AemParams& P, const DsnTabs& T, bool
 // Read-only data goes through the non-coherent path so the loads of the
 // next plane can issue ahead of this plane's stores.
 template <typename R>
-__global__ void __launch_bounds__(256, 5) k_dsn_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
+__global__ void __launch_bounds__(256, 4) k_dsn_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
     __shared__ DsnTabs T;
     load_tabs(P, T);
@@ -287,13 +287,28 @@ __global__ void __launch_bounds__(256, 5) k_dsn_h(const __grid_constant__ AemPar
     const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
     long long c = lin(P, px, py, pz0);
     R ex = ldg(Ex + c), ey = ldg(Ey + c);
+    // the loads of a plane: issued one plane ahead of its arithmetic, so two
+    // planes of requests are in flight per thread
+    struct Plane {
+        R ez, ex_jp, ex_kp, ey_ip, ey_kp, ez_ip, ez_jp, hx, hy, hz;
+    };
+    auto load = [&](long long cc) {
+        Plane p;
+        p.ez = ldg(Ez + cc);
+        p.ex_jp = ldg(Ex + cc + PX); p.ex_kp = ldg(Ex + cc + PL); p.ey_ip = ldg(Ey + cc + 1); p.ey_kp = ldg(Ey + cc + PL);
+        p.ez_ip = ldg(Ez + cc + 1); p.ez_jp = ldg(Ez + cc + PX);
+        p.hx = ldg(Hx + cc); p.hy = ldg(Hy + cc); p.hz = ldg(Hz + cc);
+        return p;
+    };
+    Plane cur = load(c);
     for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
+        Plane nxt = cur;
+        if (pz < pz_end) nxt = load(c + PL);
         const int k = pz + 1;
         const float dhz = P.den_h[2][k - 1];
-        const R ez = ldg(Ez + c);
-        const R ex_jp = ldg(Ex + c + PX), ex_kp = ldg(Ex + c + PL), ey_ip = ldg(Ey + c + 1), ey_kp = ldg(Ey + c + PL);
-        const R ez_ip = ldg(Ez + c + 1), ez_jp = ldg(Ez + c + PX);
-        R hxv = ldg(Hx + c), hyv = ldg(Hy + c), hzv = ldg(Hz + c);
+        const R ez = cur.ez, ex_jp = cur.ex_jp, ex_kp = cur.ex_kp, ey_ip = cur.ey_ip, ey_kp = cur.ey_kp;
+        const R ez_ip = cur.ez_ip, ez_jp = cur.ez_jp;
+        R hxv = cur.hx, hyv = cur.hy, hzv = cur.hz;
         hxv = hxv + DB * ((ez - ez_jp) * dhy + (ey_kp - ey) * dhz);
         hyv = hyv + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
         hzv = hzv + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
@@ -317,6 +332,7 @@ __global__ void __launch_bounds__(256, 5) k_dsn_h(const __grid_constant__ AemPar
         Hz[c] = hzv;
         ex = ex_kp;
         ey = ey_kp;
+        cur = nxt;
     }
 }
 
@@ -644,7 +660,7 @@ __device__ __forceinline__ bool h_slab(const AemParams& P, int ax, int r) {
 // E_e = Ga E_e + Gb (d1 den1 + d2 den2) (+ Gb psi), so the adjoint of its
 // difference d is den w_e (+ c/dl se), scattered to the two faces of d.
 template <typename R>
-__global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
+__global__ void __launch_bounds__(256, 4) k_adj_h(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
     __shared__ DsnTabs T;
     load_tabs(P, T);
@@ -664,14 +680,26 @@ __global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AemPar
     const int pz0 = blockIdx.z * DZCH, pz_end = min(P.SZ - 2, pz0 + DZCH - 1);
     long long c = lin(P, px, py, pz0);
     R wx0 = ldg(wX + c), wy0 = ldg(wY + c);
+    struct Plane {
+        R wxk, wyk, wz0, wxj, wyi, wzi, wzj, lx, ly, lz;
+    };
+    auto load = [&](long long cc) {
+        Plane p;
+        p.wxk = ldg(wX + cc + PL); p.wyk = ldg(wY + cc + PL); p.wz0 = ldg(wZ + cc);
+        p.wxj = ldg(wX + cc + PX); p.wyi = ldg(wY + cc + 1); p.wzi = ldg(wZ + cc + 1); p.wzj = ldg(wZ + cc + PX);
+        p.lx = ldg(lHx + cc); p.ly = ldg(lHy + cc); p.lz = ldg(lHz + cc);
+        return p;
+    };
+    Plane cur = load(c);
     for (int pz = pz0; pz <= pz_end; pz++, c += PL) {
+        Plane nxt = cur;
+        if (pz < pz_end) nxt = load(c + PL);
         const int k = pz + 1;
         const float dez0 = P.den_e[2][pz], dez1 = P.den_e[2][pz + 1];
-        const R wxk = ldg(wX + c + PL), wyk = ldg(wY + c + PL), wz0 = ldg(wZ + c);
-        const R wxj = ldg(wX + c + PX), wyi = ldg(wY + c + 1), wzi = ldg(wZ + c + 1), wzj = ldg(wZ + c + PX);
-        R lx = ldg(lHx + c) + ((dez0 * wy0 - dez1 * wyk) - (dey0 * wz0 - dey1 * wzj));
-        R ly = ldg(lHy + c) + ((dez1 * wxk - dez0 * wx0) + (dex0 * wz0 - dex1 * wzi));
-        R lz = ldg(lHz + c) + ((dey0 * wx0 - dey1 * wxj) - (dex0 * wy0 - dex1 * wyi));
+        const R wxk = cur.wxk, wyk = cur.wyk, wz0 = cur.wz0, wxj = cur.wxj, wyi = cur.wyi, wzi = cur.wzi, wzj = cur.wzj;
+        R lx = cur.lx + ((dez0 * wy0 - dez1 * wyk) - (dey0 * wz0 - dey1 * wzj));
+        R ly = cur.ly + ((dez1 * wxk - dez0 * wx0) + (dex0 * wz0 - dex1 * wzi));
+        R lz = cur.lz + ((dey0 * wx0 - dey1 * wxj) - (dex0 * wy0 - dex1 * wyi));
         if (e_slab(P, 2, pz + 1) || e_slab(P, 2, pz + 2)) {  // z differences: Ey (Hx), Ex (Hy)
             lx = lx + (pml_d(P, T, D, 1, 2, px, py, pz) - pml_d(P, T, D, 1, 2, px, py, pz + 1));
             ly = ly + (pml_d(P, T, D, 0, 2, px, py, pz + 1) - pml_d(P, T, D, 0, 2, px, py, pz));
@@ -705,6 +733,7 @@ __global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AemPar
         }
         wx0 = wxk;
         wy0 = wyk;
+        cur = nxt;
     }
 }
 
