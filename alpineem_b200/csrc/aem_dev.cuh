@@ -68,6 +68,39 @@ __device__ __forceinline__ float cpml_div(float num, float dl) {
 }
 __device__ __forceinline__ cf cpml_div(cf num, float dl) { return {cpml_div(num.x, dl), cpml_div(num.y, dl)}; }
 
+// Per-block copies of the small tables the volume kernels index per cell:
+// uniform-edge Ga/Gb and cell eps/sigma per material, CPML b/c per slab
+// depth.  Shared memory keeps the id -> coefficient lookup off the global
+// memory latency chain and serves lanes at different CPML depths in one
+// access (the same values, so results are unchanged).
+struct CoefTabs {
+    float ga[AEM_MAX_MATERIALS][3], gb[AEM_MAX_MATERIALS][3];
+    float eps[AEM_MAX_MATERIALS][3], sig[AEM_MAX_MATERIALS][3];
+    float be[3][2][AEM_MAX_PML], ce[3][2][AEM_MAX_PML], bh[3][2][AEM_MAX_PML], ch[3][2][AEM_MAX_PML];
+};
+
+// fill the block's tables; every thread of the block must call it (it ends
+// with a barrier), before any thread leaves the kernel
+__device__ inline void load_coef_tabs(const AemParams& P, CoefTabs& T) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int q = tid; q < P.nmat * 3; q += nt) {
+        const int m = q / 3, c = q % 3;
+        T.ga[m][c] = P.ucoef[m].ga[c];
+        T.gb[m][c] = P.ucoef[m].gb[c];
+        T.eps[m][c] = P.mat[m].eps[c];
+        T.sig[m][c] = P.mat[m].sig[c];
+    }
+    for (int q = tid; q < 3 * 2 * AEM_MAX_PML; q += nt) {
+        const int a = q / (2 * AEM_MAX_PML), sd = (q / AEM_MAX_PML) % 2, d = q % AEM_MAX_PML;
+        if (d >= P.npml[a][sd]) continue;
+        T.be[a][sd][d] = P.be[a][sd][d];
+        T.ce[a][sd][d] = P.ce[a][sd][d];
+        T.bh[a][sd][d] = P.bh[a][sd][d];
+        T.ch[a][sd][d] = P.ch[a][sd][d];
+    }
+    __syncthreads();
+}
+
 // the step number of this launch: the device counter during graph replay,
 // else the launch argument
 __device__ __forceinline__ int step_of(const AemParams& P, int counter) { return P.dstep ? *P.dstep : counter; }

@@ -51,11 +51,13 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
 }
 
 // z planes per CTA of the two-kernel path: a grid narrow in x and y (a
-// kmax unit cell) still spreads over every SM
+// kmax unit cell) still spreads over every SM.  (Fewer planes per CTA make
+// a single narrow run faster but leave concurrent runs of a batch less room
+// to overlap: the batched constant-k sweep lost 10 %.)
 constexpr int UPD_ZCH = 16;
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemParams P, int counter) {
+__global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 1) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * 8 + threadIdx.y;
@@ -64,6 +66,8 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
     const int hx = P.per[0] ? P.SX - 1 : P.SX - 2;
     const int hy = P.per[1] ? P.SY - 1 : P.SY - 2;
     const int hz = P.per[2] ? P.SZ - 1 : P.SZ - 2;
+    __shared__ CoefTabs Tb;
+    load_coef_tabs(P, Tb);
     if (px > hx || py > hy) return;
     const void *Ex = P.E[0], *Ey = P.E[1], *Ez = P.E[2];
     void *Hx = P.H[0], *Hy = P.H[1], *Hz = P.H[2];
@@ -214,18 +218,18 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ AemPar
         if (P.cpml_split != 1) {
             const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0;
             const int qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-            if (qy_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-            if (qy_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-            if (qz_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-            if (qz_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-            if (qx_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-            if (qx_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-            if (qz_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][0], P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-            if (qz_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][1], P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-            if (qx_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][0], P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-            if (qx_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][1], P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-            if (qy_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][0], P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-            if (qy_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][1], P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+            if (qy_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][0], Tb.bh[1][0][qy_lo - 1], Tb.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][1], Tb.bh[1][1][qy_hi - 1], Tb.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
+            if (qz_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][0], Tb.bh[2][0][qz_lo - 1], Tb.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][1], Tb.bh[2][1][qz_hi - 1], Tb.ch[2][1][qz_hi - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][0], Tb.bh[0][0][qx_lo - 1], Tb.ch[0][0][qx_lo - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][0][1], Tb.bh[0][1][qx_hi - 1], Tb.ch[0][1][qx_hi - 1], ez_ip - ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qz_lo) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][0], Tb.bh[2][0][qz_lo - 1], Tb.ch[2][0][qz_lo - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
+            if (qz_hi) hyv = hyv + DB * cpml_term<T>(P, P.psi_h[1][2][1], Tb.bh[2][1][qz_hi - 1], Tb.ch[2][1][qz_hi - 1], ex - ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
+            if (qx_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][0], Tb.bh[0][0][qx_lo - 1], Tb.ch[0][0][qx_lo - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
+            if (qx_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][0][1], Tb.bh[0][1][qx_hi - 1], Tb.ch[0][1][qx_hi - 1], ey - ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
+            if (qy_lo) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][0], Tb.bh[1][0][qy_lo - 1], Tb.ch[1][0][qy_lo - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
+            if (qy_hi) hzv = hzv + DB * cpml_term<T>(P, P.psi_h[2][1][1], Tb.bh[1][1][qy_hi - 1], Tb.ch[1][1][qy_hi - 1], ex_jp - ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
         }
         st<T>(Hx, c, hxv);
         st<T>(Hy, c, hyv);
@@ -257,8 +261,8 @@ __device__ inline void drude_coef(const AemParams& P, int c, const EdgeCoef& co,
     jb = d_jb(w, g, P.dt);
 }
 
-__device__ inline void edge_coef(const AemParams& P, int c, int px, int py, int pz, int pxd, int pyd, int pzd,
-                                 bool unaveraged, EdgeCoef& o) {
+__device__ inline void edge_coef(const AemParams& P, const CoefTabs& Tb, int c, int px, int py, int pz, int pxd, int pyd,
+                                 int pzd, bool unaveraged, EdgeCoef& o) {
     if (unaveraged) {
         o.i0 = o.i1 = o.i2 = o.i3 = 0;
     } else {
@@ -271,14 +275,12 @@ __device__ inline void edge_coef(const AemParams& P, int c, int px, int py, int 
     }
     o.uni = o.i0 == o.i1 && o.i0 == o.i2 && o.i0 == o.i3;
     if (o.uni) {
-        const AemUniformCoef& u = P.ucoef[o.i0];
-        o.ga = u.ga[c];
-        o.gb = u.gb[c];
+        o.ga = Tb.ga[o.i0][c];
+        o.gb = Tb.gb[o.i0][c];
         return;
     }
-    const AemMaterial *m0 = P.mat + o.i0, *m1 = P.mat + o.i1, *m2 = P.mat + o.i2, *m3 = P.mat + o.i3;
-    const float e = (m0->eps[c] + m1->eps[c] + m2->eps[c] + m3->eps[c]) / 4.0f;
-    const float s = (m0->sig[c] + m1->sig[c] + m2->sig[c] + m3->sig[c]) / 4.0f;
+    const float e = (Tb.eps[o.i0][c] + Tb.eps[o.i1][c] + Tb.eps[o.i2][c] + Tb.eps[o.i3][c]) / 4.0f;
+    const float s = (Tb.sig[o.i0][c] + Tb.sig[o.i1][c] + Tb.sig[o.i2][c] + Tb.sig[o.i3][c]) / 4.0f;
     float tp = 0.0f;
     for (int p = 0; p < P.npoles; p++) {
         float ja, jb;
@@ -340,10 +342,12 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_update_e(const __grid_constant__ AemParams P, int counter) {
+__global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : 2) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * 8 + threadIdx.y;
+    __shared__ CoefTabs Tb;
+    load_coef_tabs(P, Tb);
     if (px >= P.SX || py >= P.SY) return;
     const void *Hx = P.H[0], *Hy = P.H[1], *Hz = P.H[2];
     void *Ex = P.E[0], *Ey = P.E[1], *Ez = P.E[2];
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(256, 2) k_update_e(const __grid_constant__ Aem
             }
             const T curl = d1 * den1 + d2 * den2;
             EdgeCoef co;
-            edge_coef(P, comp, px, py, pz, pxd, pyd, pzd, unavg, co);
+            edge_coef(P, Tb, comp, px, py, pz, pxd, pyd, pzd, unavg, co);
             float ga = co.ga, gb = co.gb;
             if (P.nsheet) sheet_override(P, comp, px, py, pz, &ga, &gb);
             const T eold = ld<T>(Ec, c);
@@ -509,10 +513,10 @@ __global__ void __launch_bounds__(256, 2) k_update_e(const __grid_constant__ Aem
             const int q2l = ax2 == 1 ? qyl : qzl, q2h = ax2 == 1 ? qyh : qzh;
             const T t1 = comp == 2 ? d1 : (comp == 0 ? d1 : d1);  // difference along ax1
             const T t2 = d2;                                     // difference along ax2
-            if (q1l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][0], P.be[ax1][0][q1l - 1], P.ce[ax1][0][q1l - 1], t1, P.del[ax1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
-            if (q1h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][1], P.be[ax1][1][q1h - 1], P.ce[ax1][1][q1h - 1], t1, P.del[ax1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
-            if (q2l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][0], P.be[ax2][0][q2l - 1], P.ce[ax2][0][q2l - 1], t2, P.del[ax2], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
-            if (q2h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][1], P.be[ax2][1][q2h - 1], P.ce[ax2][1][q2h - 1], t2, P.del[ax2], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
+            if (q1l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][0], Tb.be[ax1][0][q1l - 1], Tb.ce[ax1][0][q1l - 1], t1, P.del[ax1], psi_idx(P, ax1, q1l, px, py, pz, P.npml[ax1][0]));
+            if (q1h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax1][1], Tb.be[ax1][1][q1h - 1], Tb.ce[ax1][1][q1h - 1], t1, P.del[ax1], psi_idx(P, ax1, q1h, px, py, pz, P.npml[ax1][1]));
+            if (q2l) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][0], Tb.be[ax2][0][q2l - 1], Tb.ce[ax2][0][q2l - 1], t2, P.del[ax2], psi_idx(P, ax2, q2l, px, py, pz, P.npml[ax2][0]));
+            if (q2h) e = e + gb * cpml_term<T>(P, P.psi_e[comp][ax2][1], Tb.be[ax2][1][q2h - 1], Tb.ce[ax2][1][q2h - 1], t2, P.del[ax2], psi_idx(P, ax2, q2h, px, py, pz, P.npml[ax2][1]));
             st<T>(Ec, c, e);
         }
     }
