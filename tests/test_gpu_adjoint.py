@@ -13,8 +13,6 @@ it meets central differences to the difference's own truncation (measured
 ~1e-7; bound 1e-5).  The FP32 adjoint of the FP32 loop (the reference's
 arithmetic) meets them to 1e-3 relative, the north-star tolerance, on every
 cell whose derivative is above 1 % of the largest checked one."""
-import os
-
 import numpy as np
 import pytest
 
