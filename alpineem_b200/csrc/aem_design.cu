@@ -1215,11 +1215,14 @@ double DsnImpl<R>::forward(int K, double dft[2]) {
 // s-1 is recomputed on the side stream while segment s is swept: the sweep
 // reads only its record buffer, the recompute writes the forward state and
 // the other buffer.  Events order each recompute after the sweep that last
-// read its buffer, and each sweep after its recompute.
+// read its buffer, and each sweep after its recompute.  The two streams'
+// launches are enqueued in alternating chunks, so neither waits behind the
+// other's backlog in the launch queue.
 template <typename R>
 void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     if (!ready_) throw std::invalid_argument("design gradient: run forward() with checkpoints first");
     const int N = steps_, K = K_, S = nseg_;
+    constexpr int CHUNK = 16;  // steps per stream per enqueue turn
     zero(adj_);
     DSN_CUDA(cudaMemsetAsync(D_.A, 0, D_.nedge * sizeof(double), st_));
     DSN_CUDA(cudaMemsetAsync(D_.B, 0, D_.nedge * sizeof(double), st_));
@@ -1228,30 +1231,43 @@ void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     launches_[1] = 0;
     auto ev_sweep = [&](int s) { return seg_event(2 * (size_t)s); };
     auto ev_rec = [&](int s) { return seg_event(2 * (size_t)s + 1); };
-    auto sweep = [&](int s) {
-        const DsnDev<R> D = with_rec(s);
-        const int s0 = s * K, s1 = std::min(s0 + K, N);
-        for (int n = s1; n > s0; n--) adj_step(n, s0, D);
-        DSN_CUDA(cudaEventRecord(ev_sweep(s), st_));
-    };
     if (!last_recorded_) {
-        recompute(S - 1, with_rec(S - 1), st_);
+        recompute(S - 1, with_rec(S - 1), st_);  // same stream as its sweep
         DSN_CUDA(cudaEventRecord(ev_rec(S - 1), st_));
-        DSN_CUDA(cudaStreamWaitEvent(sb_, ev_rec(S - 1), 0));
+        DSN_CUDA(cudaStreamWaitEvent(sb_, ev_rec(S - 1), 0));  // both write the forward state
     }
-    if (S >= 2) {
-        recompute(S - 2, with_rec(S - 2), sb_);
-        DSN_CUDA(cudaEventRecord(ev_rec(S - 2), sb_));
-    }
-    sweep(S - 1);
-    for (int s = S - 2; s >= 0; s--) {
-        if (s >= 1) {
-            DSN_CUDA(cudaStreamWaitEvent(sb_, ev_sweep(s + 1), 0));
-            recompute(s - 1, with_rec(s - 1), sb_);
-            DSN_CUDA(cudaEventRecord(ev_rec(s - 1), sb_));
+    for (int s = S - 1; s >= 0; s--) {
+        // recompute of segment s-1 on the side stream
+        const int r = s - 1;
+        const DsnDev<R> Dr = with_rec(r >= 0 ? r : 0);
+        int rn = 0, r1 = -1, r0 = 0;
+        if (r >= 0) {
+            if (s + 1 < S) DSN_CUDA(cudaStreamWaitEvent(sb_, ev_sweep(s + 1), 0));
+            r0 = r * K;
+            r1 = std::min(r0 + K, N);
+            const char* src = ck_ + (size_t)r * state_bytes_;
+            for (auto& a : state_) {
+                DSN_CUDA(cudaMemcpyAsync(a.first, src, a.second, cudaMemcpyDeviceToDevice, sb_));
+                src += (a.second + 255) / 256 * 256;
+            }
+            k_dsn_record<R><<<egrid(Dr.nedge), 256, 0, sb_>>>(P_, Dr, 0);
+            launches_[1]++;
+            rn = r0 + 1;
         }
-        DSN_CUDA(cudaStreamWaitEvent(st_, ev_rec(s), 0));
-        sweep(s);
+        // sweep of segment s on the run's stream, after its recompute
+        if (s < S - 1) DSN_CUDA(cudaStreamWaitEvent(st_, ev_rec(s), 0));
+        const DsnDev<R> Da = with_rec(s);
+        const int s0 = s * K;
+        int an = std::min(s0 + K, N);
+        while (rn <= r1 || an > s0) {
+            for (int q = 0; q < CHUNK && rn <= r1; q++, rn++) {
+                step(rn, rn - r0, 0, Dr, sb_);
+                launches_[1] += 4;
+            }
+            for (int q = 0; q < CHUNK && an > s0; q++, an--) adj_step(an, s0, Da);
+        }
+        if (r >= 0) DSN_CUDA(cudaEventRecord(ev_rec(r), sb_));
+        DSN_CUDA(cudaEventRecord(ev_sweep(s), st_));
     }
     last_recorded_ = false;  // earlier segments' recomputes overwrote the records
     const long long ncell = (long long)D_.n[0] * D_.n[1] * D_.n[2];
