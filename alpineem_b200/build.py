@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -fmad=false: FP32 results round like the reference's expressions;
 # -ftz=true: subnormals flush to zero, as in the reference's Intel -O3 builds
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-ftz=true", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + ARCH
-CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-I" + os.path.join(CUDA_HOME, "include")]
+CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-pthread", "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU = ["aem_kernels.cu", "aem_yee.cu", "aem_yee4.cu", "aem_aux.cu", "aem_dft.cu", "aem_dft_static.cu", "aem_solver.cu", "aem_finalize.cu", "aem_design.cu"]
 CPP = ["aem_deck.cpp", "aem_model.cpp", "aem_api.cpp"]
@@ -69,7 +69,7 @@ def build(verbose=False):
     objs = [os.path.join(OBJ, f + ".o") for f in CU + CPP]
     so = os.path.join(LIB, "libalpineem_b200.so")
     if _stale(so, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart"])
+        _run([NVCC] + ARCH + ["-shared", "-o", so] + objs + ["-lcudart", "-Xcompiler", "-pthread"])
     exe = os.path.join(LIB, "FDTD-B200")
     main = os.path.join(SRC, "fdtd_b200_main.cpp")
     if _stale(exe, [main, so]):

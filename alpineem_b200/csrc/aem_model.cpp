@@ -13,13 +13,34 @@
 #include "aem_model.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <thread>
 
 namespace aem {
+
+// f(0..n-1) on the host's cores (items handed out one at a time); for
+// loops whose iterations write disjoint data
+template <typename F>
+static void par_for(int n, F&& f) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<unsigned>(hc ? hc : 1, 64);
+    if (n < 16 || nt <= 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < std::min(nt, n); t++)
+        th.emplace_back([&] {
+            for (int i; (i = next.fetch_add(1)) < n;) f(i);
+        });
+    for (auto& x : th) x.join();
+}
 namespace {
 
 constexpr float kEp0 = 8.85418782E-12f;
@@ -160,7 +181,9 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
         return true;
     };
 
-    m.cell_id.assign((size_t)m.cells, 0);
+    m.cell_id.clear();
+    m.cell_id.resize((size_t)m.cells);  // uninitialised: zeroed plane by plane in parallel
+    par_for(m.S[2], [&](int z) { std::memset(m.cell_id.data() + (size_t)z * m.plane, 0, (size_t)m.plane); });
     if (!d.bulk_file.empty()) {  // ref :2051-2095
         const size_t nbulk = (size_t)gx * gy * gz;
         std::vector<float> file_data;
@@ -181,7 +204,8 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
         for (auto& vm : d.mats) mx = std::max(mx, (int)vm.id);
         std::vector<int> tmp((size_t)mx + 1, 0);
         for (size_t r = 0; r < d.mats.size(); r++) tmp[(int)d.mats[r].id] = (int)r + 1;
-        for (int k = 1; k <= gz; k++)
+        par_for(gz, [&](int kk) {  // planes write disjoint cells
+            const int k = kk + 1;
             for (int j = 1; j <= gy; j++)
                 for (int i = 1; i <= gx; i++) {
                     float v = bg[((size_t)(k - 1) * gy + (j - 1)) * gx + (i - 1)];
@@ -190,6 +214,7 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
                     if (mid != 0) m.cell_id[m.lin(i, j, k)] = (uint8_t)mid;
                     if (float* g = geo(0, i, j, k)) *g = v;
                 }
+        });
     }
     int mid = 0;
     for (auto& o : d.objects) {  // ref :2101-2288

@@ -3,7 +3,9 @@
 #pragma once
 #include <stdint.h>
 
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "aem_deck.h"
@@ -18,12 +20,30 @@ struct SheetPlaneHost {
     std::vector<float> sa, sb, ga1, gb1, ga2, gb2;
 };
 
+// std::allocator that leaves new elements uninitialised (resize() of a
+// multi-GB array need not write it; the model builder fills it in parallel)
+template <typename T>
+struct DefaultInit : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = DefaultInit<U>;
+    };
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+
 struct HostModel {
     Deck d;
     int S[3] = {0, 0, 0};   // storage extents per axis
     int PX = 0;             // x pitch
     long long plane = 0, cells = 0;
-    std::vector<uint8_t> cell_id;                 // [SZ][SY][PX], 0 = vacuum
+    std::vector<uint8_t, DefaultInit<uint8_t>> cell_id;  // [SZ][SY][PX], 0 = vacuum
     std::vector<AemMaterial> mats;                // 0 = vacuum, 1.. = deck volume materials
     std::vector<AemUniformCoef> ucoef;            // same indexing
     int npoles = 0;

@@ -51,8 +51,8 @@ void* Solver::alloc(size_t bytes) {
     return p;
 }
 
-template <typename V>
-void* Solver::upload(const std::vector<V>& v) {
+template <typename V, typename A>
+void* Solver::upload(const std::vector<V, A>& v) {
     void* p = alloc(v.size() * sizeof(V));
     if (!v.empty()) AEM_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, stream_));
     h2d_bytes_ += v.size() * sizeof(V);

@@ -98,8 +98,8 @@ class Solver {
     void init();
     void release();
     void* alloc(size_t bytes);
-    template <typename V>
-    void* upload(const std::vector<V>& v);
+    template <typename V, typename A>
+    void* upload(const std::vector<V, A>& v);
     void setup_params();
     void setup_ports();
     void setup_farfield();
