@@ -327,7 +327,7 @@ __device__ __forceinline__ R dsn_e1(const AemParams& P, const DsnTabs& T, const 
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256, 5) k_dsn_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int slot) {
+__global__ void __launch_bounds__(256, 4) k_dsn_e(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int slot) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
     __shared__ DsnTabs T;
     load_tabs(P, T);
@@ -361,6 +361,11 @@ __global__ void __launch_bounds__(256, 5) k_dsn_e(const __grid_constant__ AemPar
         const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
         const bool pml = colpml || qzl || qzh;
         const R hx = ldg(Hx + c), hy = ldg(Hy + c), hz = ldg(Hz + c);
+        // the rest of the plane's loads, issued before any update so that a
+        // thread waits on one round of memory latency
+        const R ex_o = ldg(Ex + c), ey_o = ldg(Ey + c), ez_o = ldg(Ez + c);
+        const R hz_jm = yok ? ldg(Hz + c - PX) : R(0), hx_jm = yok ? ldg(Hx + c - PX) : R(0);
+        const R hz_im = xok ? ldg(Hz + c - 1) : R(0), hy_im = xok ? ldg(Hy + c - 1) : R(0);
         R ga[3], gb[3];
         coef3(P, T, unavg_col || pz == 0, a, b, ga, gb);
         const bool dsn = coldsn && pz >= D.lo[2] && pz <= D.lo[2] + D.n[2];
@@ -370,17 +375,17 @@ __global__ void __launch_bounds__(256, 5) k_dsn_e(const __grid_constant__ AemPar
                 if (dsn_edge(D, cc, px, py, pz, &q[cc])) { ga[cc] = D.ga[q[cc]]; gb[cc] = D.gb[q[cc]]; }
                 else q[cc] = -1;
         if (yok && pz >= 1) {
-            const R e = dsn_e1(P, T, D, 0, ldg(Ex + c), hz - ldg(Hz + c - PX), hy_m - hy, dey, dez, ga[0], gb[0], pml, qyl, qyh, qzl, qzh, px, py, pz);
+            const R e = dsn_e1(P, T, D, 0, ex_o, hz - hz_jm, hy_m - hy, dey, dez, ga[0], gb[0], pml, qyl, qyh, qzl, qzh, px, py, pz);
             Ex[c] = e;
             if (slot >= 0 && q[0] >= 0) D.rec[slot * D.nedge + q[0]] = e;
         }
         if (xok && pz >= 1) {
-            const R e = dsn_e1(P, T, D, 1, ldg(Ey + c), ldg(Hz + c - 1) - hz, hx - hx_m, dex, dez, ga[1], gb[1], pml, qxl, qxh, qzl, qzh, px, py, pz);
+            const R e = dsn_e1(P, T, D, 1, ey_o, hz_im - hz, hx - hx_m, dex, dez, ga[1], gb[1], pml, qxl, qxh, qzl, qzh, px, py, pz);
             Ey[c] = e;
             if (slot >= 0 && q[1] >= 0) D.rec[slot * D.nedge + q[1]] = e;
         }
         if (xok && yok) {
-            const R e = dsn_e1(P, T, D, 2, ldg(Ez + c), hy - ldg(Hy + c - 1), ldg(Hx + c - PX) - hx, dex, dey, ga[2], gb[2], pml, qxl, qxh, qyl, qyh, px, py, pz);
+            const R e = dsn_e1(P, T, D, 2, ez_o, hy - hy_im, hx_jm - hx, dex, dey, ga[2], gb[2], pml, qxl, qxh, qyl, qyh, px, py, pz);
             Ez[c] = e;
             if (slot >= 0 && q[2] >= 0) D.rec[slot * D.nedge + q[2]] = e;
         }
@@ -713,9 +718,9 @@ __global__ void __launch_bounds__(256, 4) k_adj_h(const __grid_constant__ AemPar
 // per edge is w = Gb lE (Gb > 0 for every material), so lE = Ga lE + g
 // becomes w = Ga w + Gb g; then se = b se + w on its CPML slabs
 template <typename R>
-__device__ __forceinline__ void adj_e1(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, long long c, R g, R ga, R gb,
-                                       bool pml, int q1l, int q1h, int q2l, int q2h, int px, int py, int pz) {
-    const R wv = ga * ldg(D.w[comp] + c) + gb * g;
+__device__ __forceinline__ void adj_e1(const AemParams& P, const DsnTabs& T, const DsnDev<R>& D, int comp, long long c, R wold, R g,
+                                       R ga, R gb, bool pml, int q1l, int q1h, int q2l, int q2h, int px, int py, int pz) {
+    const R wv = ga * wold + gb * g;
     D.w[comp][c] = wv;
     if (pml) {
         const int ax1 = comp == 0 ? 1 : 0, ax2 = comp == 2 ? 1 : 2;
@@ -771,6 +776,10 @@ __global__ void __launch_bounds__(256, 5) k_adj_e(const __grid_constant__ AemPar
         const bool pe = colpe || qzl || qzh;
         const bool phz = h_slab(P, 2, pz + 1) || h_slab(P, 2, pz);
         const R lx = ldg(lHx + c), ly = ldg(lHy + c), lz = ldg(lHz + c);
+        // the -x / -y neighbours, issued with the others before any update
+        const R lz_jm = yok ? ldg(lHz + c - PX) : R(0), lx_jm = yok ? ldg(lHx + c - PX) : R(0);
+        const R lz_im = xok ? ldg(lHz + c - 1) : R(0), ly_im = xok ? ldg(lHy + c - 1) : R(0);
+        const R w0 = ldg(D.w[0] + c), w1 = ldg(D.w[1] + c), w2 = ldg(D.w[2] + c);
         R ga[3], gb[3];
         coef3(P, T, unavg_col || pz == 0, a, b, ga, gb);
         if (coldsn && pz >= D.lo[2] && pz <= D.lo[2] + D.n[2])
@@ -779,22 +788,22 @@ __global__ void __launch_bounds__(256, 5) k_adj_e(const __grid_constant__ AemPar
                 if (dsn_edge(D, cc, px, py, pz, &q)) { ga[cc] = D.ga[q]; gb[cc] = D.gb[q]; }
             }
         if (yok && pz >= 1) {  // Ex: d1 = Hz - Hz[j-1] (y), d2 = Hy[k-1] - Hy (z)
-            R g = (bz0 * ly - bzm * ly_m) + (bym * ldg(lHz + c - PX) - by0 * lz);
+            R g = (bz0 * ly - bzm * ly_m) + (bym * lz_jm - by0 * lz);
             if (phz) g = g + (pml_m(P, T, D, 1, 2, px, py, pz) - pml_m(P, T, D, 1, 2, px, py, pz - 1));
             if (phy) g = g + (pml_m(P, T, D, 2, 1, px, py - 1, pz) - pml_m(P, T, D, 2, 1, px, py, pz));
-            adj_e1(P, T, D, 0, c, g, ga[0], gb[0], pe, qyl, qyh, qzl, qzh, px, py, pz);
+            adj_e1(P, T, D, 0, c, w0, g, ga[0], gb[0], pe, qyl, qyh, qzl, qzh, px, py, pz);
         }
         if (xok && pz >= 1) {  // Ey: d1 = Hz[i-1] - Hz (x), d2 = Hx - Hx[k-1] (z)
-            R g = (bzm * lx_m - bz0 * lx) + (bx0 * lz - bxm * ldg(lHz + c - 1));
+            R g = (bzm * lx_m - bz0 * lx) + (bx0 * lz - bxm * lz_im);
             if (phz) g = g + (pml_m(P, T, D, 0, 2, px, py, pz - 1) - pml_m(P, T, D, 0, 2, px, py, pz));
             if (phx) g = g + (pml_m(P, T, D, 2, 0, px, py, pz) - pml_m(P, T, D, 2, 0, px - 1, py, pz));
-            adj_e1(P, T, D, 1, c, g, ga[1], gb[1], pe, qxl, qxh, qzl, qzh, px, py, pz);
+            adj_e1(P, T, D, 1, c, w1, g, ga[1], gb[1], pe, qxl, qxh, qzl, qzh, px, py, pz);
         }
         if (xok && yok) {  // Ez: d1 = Hy - Hy[i-1] (x), d2 = Hx[j-1] - Hx (y)
-            R g = (by0 * lx - bym * ldg(lHx + c - PX)) + (bxm * ldg(lHy + c - 1) - bx0 * ly);
+            R g = (by0 * lx - bym * lx_jm) + (bxm * ly_im - bx0 * ly);
             if (phy) g = g + (pml_m(P, T, D, 0, 1, px, py, pz) - pml_m(P, T, D, 0, 1, px, py - 1, pz));
             if (phx) g = g + (pml_m(P, T, D, 1, 0, px - 1, py, pz) - pml_m(P, T, D, 1, 0, px, py, pz));
-            adj_e1(P, T, D, 2, c, g, ga[2], gb[2], pe, qxl, qxh, qyl, qyh, px, py, pz);
+            adj_e1(P, T, D, 2, c, w2, g, ga[2], gb[2], pe, qxl, qxh, qyl, qyh, px, py, pz);
         }
         lx_m = lx;
         ly_m = ly;

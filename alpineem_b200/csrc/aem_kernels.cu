@@ -261,18 +261,11 @@ __device__ inline void drude_coef(const AemParams& P, int c, const EdgeCoef& co,
     jb = d_jb(w, g, P.dt);
 }
 
-__device__ inline void edge_coef(const AemParams& P, const CoefTabs& Tb, int c, int px, int py, int pz, int pxd, int pyd,
-                                 int pzd, bool unaveraged, EdgeCoef& o) {
-    if (unaveraged) {
-        o.i0 = o.i1 = o.i2 = o.i3 = 0;
-    } else {
-        // four cells around the edge, ref :2516-2527
-        const uint8_t* C = P.cell;
-        o.i0 = C[lin(P, px, py, pz)];
-        if (c == 0) { o.i1 = C[lin(P, px, pyd, pz)]; o.i2 = C[lin(P, px, py, pzd)]; o.i3 = C[lin(P, px, pyd, pzd)]; }
-        else if (c == 1) { o.i1 = C[lin(P, pxd, py, pz)]; o.i2 = C[lin(P, px, py, pzd)]; o.i3 = C[lin(P, pxd, py, pzd)]; }
-        else { o.i1 = C[lin(P, pxd, py, pz)]; o.i2 = C[lin(P, px, pyd, pz)]; o.i3 = C[lin(P, pxd, pyd, pz)]; }
-    }
+// i0..i3: the ids of the four cells around the edge in the reference's
+// order (ref :2516-2527), all 0 on an unaveraged wall edge
+__device__ inline void edge_coef(const AemParams& P, const CoefTabs& Tb, int c, int i0, int i1, int i2, int i3,
+                                 EdgeCoef& o) {
+    o.i0 = i0; o.i1 = i1; o.i2 = i2; o.i3 = i3;
     o.uni = o.i0 == o.i1 && o.i0 == o.i2 && o.i0 == o.i3;
     if (o.uni) {
         o.ga = Tb.ga[o.i0][c];
@@ -387,35 +380,48 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : 2) k_upd
         const int riz_t = rep_idx(P, 2, pz, true);
         const float dez = P.den_e[2][k - 1];
         const bool unavg = x_unavg || y_unavg || (!P.per[2] && k == 1);
-        const long long c = lin(P, px, py, pz);
-        const T hx = ld<T>(Hx, c), hy = ld<T>(Hy, c), hz = ld<T>(Hz, c);
         const int qzl = (k >= 2 && k <= P.npml[2][0]) ? k : 0, qzh = (k >= P.Z + 1 - P.npml[2][1] && k <= P.Z - 1) ? P.Z + 1 - k : 0;
+        // Every global load of the plane is issued before any update, so a
+        // thread waits on one round of memory latency instead of one per
+        // component.  A neighbour index of a component not updated here is
+        // clamped to 0 above and its value is not used.
+        const long long c = lin(P, px, py, pz);
+        const long long cxm = lin(P, pxd, py, pz), cym = lin(P, px, pyd, pz), czm = lin(P, px, py, pzd);
+        const T hx = ld<T>(Hx, c), hy = ld<T>(Hy, c), hz = ld<T>(Hz, c);
+        const T hz_jm = ld_dn<T>(P, Hz, cym, wyd, 1), hy_km = ld_dn<T>(P, Hy, czm, wzd, 2);
+        const T hz_im = ld_dn<T>(P, Hz, cxm, wxd, 0), hx_km = ld_dn<T>(P, Hx, czm, wzd, 2);
+        const T hy_im = ld_dn<T>(P, Hy, cxm, wxd, 0), hx_jm = ld_dn<T>(P, Hx, cym, wyd, 1);
+        const T eo0 = ld<T>(Ex, c), eo1 = ld<T>(Ey, c), eo2 = ld<T>(Ez, c);
+        // the seven cells around this position's three edges, ref :2516-2527
+        int id0 = 0, idx = 0, idy = 0, idz = 0, idxy = 0, idxz = 0, idyz = 0;
+        if (!unavg) {
+            const uint8_t* C = P.cell;
+            id0 = C[c]; idx = C[cxm]; idy = C[cym]; idz = C[czm];
+            idxy = C[lin(P, pxd, pyd, pz)]; idxz = C[lin(P, pxd, py, pzd)]; idyz = C[lin(P, px, pyd, pzd)];
+        }
 
+#pragma unroll
         for (int comp = 0; comp < 3; comp++) {
             if ((comp == 0 && !ex_u) || (comp == 1 && !ey_u) || (comp == 2 && !ez_u)) continue;
             void* Ec = P.E[comp];
             // curl of H, ref :5673-5705
             T d1, d2;   // the two difference terms (second minus first neighbour as in the reference)
             float den1, den2;
+            EdgeCoef co;
             if (comp == 0) {
-                const T hz_jm = ld_dn<T>(P, Hz, lin(P, px, pyd, pz), wyd, 1);
-                const T hy_km = ld_dn<T>(P, Hy, lin(P, px, py, pzd), wzd, 2);
                 d1 = hz - hz_jm; den1 = dey; d2 = hy_km - hy; den2 = dez;
+                edge_coef(P, Tb, 0, id0, idy, idz, idyz, co);
             } else if (comp == 1) {
-                const T hz_im = ld_dn<T>(P, Hz, lin(P, pxd, py, pz), wxd, 0);
-                const T hx_km = ld_dn<T>(P, Hx, lin(P, px, py, pzd), wzd, 2);
                 d1 = hz_im - hz; den1 = dex; d2 = hx - hx_km; den2 = dez;
+                edge_coef(P, Tb, 1, id0, idx, idz, idxz, co);
             } else {
-                const T hy_im = ld_dn<T>(P, Hy, lin(P, pxd, py, pz), wxd, 0);
-                const T hx_jm = ld_dn<T>(P, Hx, lin(P, px, pyd, pz), wyd, 1);
                 d1 = hy - hy_im; den1 = dex; d2 = hx_jm - hx; den2 = dey;
+                edge_coef(P, Tb, 2, id0, idx, idy, idxy, co);
             }
             const T curl = d1 * den1 + d2 * den2;
-            EdgeCoef co;
-            edge_coef(P, Tb, comp, px, py, pz, pxd, pyd, pzd, unavg, co);
             float ga = co.ga, gb = co.gb;
             if (P.nsheet) sheet_override(P, comp, px, py, pz, &ga, &gb);
-            const T eold = ld<T>(Ec, c);
+            const T eold = comp == 0 ? eo0 : comp == 1 ? eo1 : eo2;
             T e = eold;
             if (P.cpml_split != 2) {
             e = ga * eold + gb * curl;
