@@ -11,6 +11,8 @@
 #include <cstring>
 #include <stdexcept>
 
+#include "aem_dev.cuh"
+#include "aem_model.h"
 #include "aem_solver.h"
 
 namespace aem {
@@ -25,6 +27,69 @@ namespace aem {
 namespace {
 
 using cplx = std::complex<float>;
+
+// Far-field rE_theta / rE_phi of one angle from its six binned components
+// (W x,y,z then U x,y,z), ref :8483-8534, in the host expression's FP32
+// operation order: Wt = (wx c1) c2 + (wy c1) s2 - wz s1, Wp = (-1 wx) s2 +
+// wy c2 (U likewise), Et = (-1 eta) Wt - Up, Ep = (-1 eta) Wp + Ut.  The
+// angle's cosines and sines come from the host.
+template <typename V>
+__device__ inline void ff_pol(const V* uw, long long stride, long long j, const float* cs, float eta, V& Et, V& Ep) {
+    const float c1 = cs[0], s1 = cs[1], c2 = cs[2], s2 = cs[3];
+    const V wx = uw[j], wy = uw[stride + j], wz = uw[2 * stride + j];
+    const V ux = uw[3 * stride + j], uy = uw[4 * stride + j], uz = uw[5 * stride + j];
+    const V Wt = wx * c1 * c2 + wy * c1 * s2 - wz * s1;
+    const V Wp = -1.0f * wx * s2 + wy * c2;
+    const V Ut = ux * c1 * c2 + uy * c1 * s2 - uz * s1;
+    const V Up = -1.0f * ux * s2 + uy * c2;
+    const float me = -1.0f * eta;
+    Et = me * Wt - Up;
+    Ep = me * Wp + Ut;
+}
+__device__ inline bool nz(float v) { return v != 0.0f; }
+__device__ inline bool nz(cf v) { return v.x != 0.0f || v.y != 0.0f; }
+
+// One CTA per angle: the first bins (1-based) where Ep and Et are non-zero
+// give the output window start o (ref :8520-8530), then the T values from o
+// are written.  UW rows: [component][angle][L]; an angle whose delays equal
+// an earlier one's reads that angle's rows (canon).
+template <typename V>
+__global__ void k_ff_out(const V* UW, int nff, long long L, int len_ff, int T, const float* trig, float eta,
+                         const int* canon, V* eth, V* eph, int* out_time) {
+    const int i = blockIdx.x;
+    const V* uw = UW + (long long)canon[i] * L;
+    const long long stride = (long long)nff * L;
+    const float* cs = trig + 4 * i;
+    __shared__ int first[2];
+    if (threadIdx.x == 0) first[0] = first[1] = len_ff;
+    __syncthreads();
+    int dp = len_ff, dt = len_ff;
+    for (int j = 1 + threadIdx.x; j <= len_ff; j += blockDim.x) {
+        if (j >= dp && j >= dt) break;
+        V Et, Ep;
+        ff_pol(uw, stride, j - 1, cs, eta, Et, Ep);
+        if (nz(Ep) && j < dp) dp = j;
+        if (nz(Et) && j < dt) dt = j;
+    }
+    atomicMin(&first[0], dp);
+    atomicMin(&first[1], dt);
+    __syncthreads();
+    int o = min(first[0], first[1]);
+    if (o > len_ff - T + 1) o = len_ff - T + 1;
+    if (threadIdx.x == 0) out_time[i] = o;
+    for (int j = 1 + threadIdx.x; j <= T; j += blockDim.x) {
+        V Et, Ep;
+        const long long b = (long long)j + o - 2;  // 0-based bin
+        if (b < 0 || b >= len_ff) {                // only when len_ff < T
+            eth[(long long)i * T + j - 1] = V();
+            eph[(long long)i * T + j - 1] = V();
+            continue;
+        }
+        ff_pol(uw, stride, b, cs, eta, Et, Ep);
+        eth[(long long)i * T + j - 1] = Et;
+        eph[(long long)i * T + j - 1] = Ep;
+    }
+}
 
 // device buffer -> host, complex or real
 std::vector<cplx> fetch(const void* dev, size_t n, bool kmax, cudaStream_t s, size_t& counter) {
@@ -127,35 +192,39 @@ void Solver::finalize_and_write() {
     std::vector<std::vector<cplx>> eth(nff), eph(nff);
     data_out_time.assign(nff, 1);
     if (nff > 0) {
+        // the transform runs on the device; only each angle's T-step window
+        // comes back
         const size_t L = FF_.len;
-        std::vector<cplx> uw = fetch(FF_.UW, 6 * (size_t)nff * L, K, stream_, d2h_bytes_);
-        for (int i = 0; i < nff && i < (int)ff_canon_.size(); i++)
-            if (ff_canon_[i] != i)
-                for (int comp = 0; comp < 6; comp++)
-                    std::copy_n(uw.begin() + ((size_t)comp * nff + ff_canon_[i]) * L, L, uw.begin() + ((size_t)comp * nff + i) * L);
         const float eta = std::sqrt(mu0 / ep0);
+        std::vector<float> trig(4 * (size_t)nff);
         for (int i = 0; i < nff; i++) {
             const float a1 = d.ff_theta[i], a2 = d.ff_phi[i];
-            std::vector<cplx> Et(d.len_ff + 1), Ep(d.len_ff + 1);
-            for (int j = 1; j <= d.len_ff; j++) {
-                auto g = [&](int comp) { return uw[((size_t)comp * nff + i) * L + (j - 1)]; };
-                cplx wx = g(0), wy = g(1), wz = g(2), ux = g(3), uy = g(4), uz = g(5);
-                cplx Wt = wx * std::cos(a1) * std::cos(a2) + wy * std::cos(a1) * std::sin(a2) - wz * std::sin(a1);
-                cplx Wp = -1.0f * wx * std::sin(a2) + wy * std::cos(a2);
-                cplx Ut = ux * std::cos(a1) * std::cos(a2) + uy * std::cos(a1) * std::sin(a2) - uz * std::sin(a1);
-                cplx Up = -1.0f * ux * std::sin(a2) + uy * std::cos(a2);
-                Et[j] = -1.0f * eta * Wt - Up;
-                Ep[j] = -1.0f * eta * Wp + Ut;
-            }
-            int dp = d.len_ff, dt = d.len_ff;
-            for (int j = 1; j <= d.len_ff; j++) if (Ep[j] != cplx(0, 0)) { dp = j; break; }
-            for (int j = 1; j <= d.len_ff; j++) if (Et[j] != cplx(0, 0)) { dt = j; break; }
-            int o = dp < dt ? dp : dt;
-            if (o > d.len_ff - T + 1) o = d.len_ff - T + 1;
-            data_out_time[i] = o;
-            eth[i].resize(T);
-            eph[i].resize(T);
-            for (int j = 1; j <= T; j++) { eth[i][j - 1] = Et[j + o - 1]; eph[i][j - 1] = Ep[j + o - 1]; }
+            trig[4 * i] = std::cos(a1); trig[4 * i + 1] = std::sin(a1);
+            trig[4 * i + 2] = std::cos(a2); trig[4 * i + 3] = std::sin(a2);
+        }
+        std::vector<int> canon(nff);
+        for (int i = 0; i < nff; i++) canon[i] = i < (int)ff_canon_.size() ? ff_canon_[i] : i;
+        float* d_trig = (float*)alloc(trig.size() * sizeof(float));
+        int* d_canon = (int*)alloc(canon.size() * sizeof(int));
+        int* d_time = (int*)alloc(canon.size() * sizeof(int));
+        void* d_eth = alloc((size_t)nff * T * es_);
+        void* d_eph = alloc((size_t)nff * T * es_);
+        AEM_CUDA(cudaMemcpyAsync(d_trig, trig.data(), trig.size() * sizeof(float), cudaMemcpyHostToDevice, stream_));
+        AEM_CUDA(cudaMemcpyAsync(d_canon, canon.data(), canon.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+        if (K)
+            k_ff_out<cf><<<nff, 256, 0, stream_>>>((const cf*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta, d_canon,
+                                                   (cf*)d_eth, (cf*)d_eph, d_time);
+        else
+            k_ff_out<float><<<nff, 256, 0, stream_>>>((const float*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta,
+                                                      d_canon, (float*)d_eth, (float*)d_eph, d_time);
+        AEM_CUDA(cudaGetLastError());
+        AEM_CUDA(cudaMemcpyAsync(data_out_time.data(), d_time, nff * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        d2h_bytes_ += nff * sizeof(int);
+        std::vector<cplx> th = fetch(d_eth, (size_t)nff * T, K, stream_, d2h_bytes_);
+        std::vector<cplx> ph = fetch(d_eph, (size_t)nff * T, K, stream_, d2h_bytes_);
+        for (int i = 0; i < nff; i++) {
+            eth[i].assign(th.begin() + (size_t)i * T, th.begin() + (size_t)(i + 1) * T);
+            eph[i].assign(ph.begin() + (size_t)i * T, ph.begin() + (size_t)(i + 1) * T);
         }
     }
     std::vector<std::vector<cplx>> vout(d.ports.size());

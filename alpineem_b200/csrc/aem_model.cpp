@@ -23,24 +23,6 @@
 
 namespace aem {
 
-// f(0..n-1) on the host's cores (items handed out one at a time); for
-// loops whose iterations write disjoint data
-template <typename F>
-static void par_for(int n, F&& f) {
-    const unsigned hc = std::thread::hardware_concurrency();
-    const int nt = (int)std::min<unsigned>(hc ? hc : 1, 64);
-    if (n < 16 || nt <= 1) {
-        for (int i = 0; i < n; i++) f(i);
-        return;
-    }
-    std::atomic<int> next{0};
-    std::vector<std::thread> th;
-    for (int t = 0; t < std::min(nt, n); t++)
-        th.emplace_back([&] {
-            for (int i; (i = next.fetch_add(1)) < n;) f(i);
-        });
-    for (auto& x : th) x.join();
-}
 namespace {
 
 constexpr float kEp0 = 8.85418782E-12f;

@@ -3,8 +3,11 @@
 #pragma once
 #include <stdint.h>
 
+#include <algorithm>
+#include <atomic>
 #include <memory>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -12,6 +15,25 @@
 #include "aem_types.h"
 
 namespace aem {
+
+// f(0..n-1) on the host's cores (items handed out one at a time); for
+// loops whose iterations write disjoint data
+template <typename F>
+inline void par_for(int n, F&& f) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<unsigned>(hc ? hc : 1, 64);
+    if (n < 16 || nt <= 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < std::min(nt, n); t++)
+        th.emplace_back([&] {
+            for (int i; (i = next.fetch_add(1)) < n;) f(i);
+        });
+    for (auto& x : th) x.join();
+}
 
 struct SheetPlaneHost {
     int axis = 0, pos = 0;        // normal axis, reference index along it
