@@ -67,6 +67,9 @@ def load_library():
     lib.aem_check_deck.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.aem_read_probe.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.aem_time_step.argtypes = [h, ctypes.POINTER(ctypes.c_double)]
+    lib.aem_read_spectrum.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.aem_profile.argtypes = [h, ctypes.c_int]
     lib.aem_profile_read.argtypes = [h, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     lib.aem_launch_count.argtypes = [h, ctypes.POINTER(ctypes.c_longlong)]
@@ -191,6 +194,13 @@ class Simulation:
         return d.value, t.value
 
     @property
+    def time_step(self):
+        """del_t in seconds."""
+        dt = ctypes.c_double()
+        self._check(self._lib.aem_time_step(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    @property
     def grid(self):
         g = (ctypes.c_int * 3)()
         self._lib.aem_grid(self._h, g)
@@ -253,6 +263,16 @@ class Simulation:
         re, im = np.zeros(n), np.zeros(n)
         self._check(self._lib.aem_read_probe(self._h, k, int(index), int(first), int(n), _dptr(re), _dptr(im)))
         return (re + 1j * im) if self.kmax else re
+
+    def spectrum(self, kind, index=0, n=4096):
+        """On-the-fly spectrum of a per-step series over the steps run so
+        far (sidecar extension `dft_freqs f_start f_stop count`):
+        X(f) = sum_m x[m] exp(-2 pi i f m dt) of the raw samples that
+        probe() returns.  Returns (freqs in Hz, complex128 array)."""
+        k = SERIES[kind] if isinstance(kind, str) else int(kind)
+        f, re, im = np.zeros(n), np.zeros(n), np.zeros(n)
+        m = self._check(self._lib.aem_read_spectrum(self._h, k, int(index), int(n), _dptr(f), _dptr(re), _dptr(im)))
+        return f[:m], re[:m] + 1j * im[:m]
 
     def profile(self, enable=True):
         """Turn per-phase event timing on (clearing the record) or off."""

@@ -262,6 +262,17 @@ int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, do
     });
 }
 
+int aem_read_spectrum(aem_handle* h, int kind, int index, int n, double* freqs, double* re, double* im) {
+    if (!h || !re || n < 0) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() { return h->s->read_spectrum(kind, index, n, freqs, re, im); });
+}
+
+int aem_time_step(aem_handle* h, double* dt) {
+    if (!h || !dt) return fail(h, AEM_ERR_ARG, "bad argument");
+    *dt = (double)h->s->model().d.del_t;
+    return AEM_OK;
+}
+
 int aem_workload(aem_handle* h, long long* cells, double* bytes_per_step) {
     if (!h) return AEM_ERR_ARG;
     if (cells) *cells = h->s->cell_count();

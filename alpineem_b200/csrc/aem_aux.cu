@@ -569,6 +569,34 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
         at<T>(D.pc[3], counter - 1) = hx; at<T>(D.pc[4], counter - 1) = hy; at<T>(D.pc[5], counter - 1) = hz;
         if (counter < steps) { at<T>(D.pc[3], counter) = hx; at<T>(D.pc[4], counter) = hy; at<T>(D.pc[5], counter) = hz; }
     }
+    if (D.ndft) {
+        // this step's samples are in place (plane sums above, port voltages
+        // from the E half-step's port kernel)
+        __syncthreads();
+        const long long m = counter - 1;
+        for (int q = tid; q < D.nser * D.ndft; q += blockDim.x) {
+            const int sr = q / D.ndft, f = q % D.ndft;
+            const T x = at<T>(const_cast<void*>(D.ser[sr]), m);
+            double xr, xi;
+            if constexpr (sizeof(T) == sizeof(float)) { xr = (double)x; xi = 0.0; }
+            else { xr = (double)x.x; xi = (double)x.y; }
+            // phase in half-turns, reduced to [0, 2) before sincospi
+            double ph = (2.0 * D.dft_f[f] * D.dft_dt) * (double)m;
+            ph -= 2.0 * floor(0.5 * ph);
+            double sn, cs;
+            sincospi(ph, &sn, &cs);
+            // (xr + i xi)(cs - i sn), added with Kahan compensation
+            const double tr = xr * cs + xi * sn, ti = xi * cs - xr * sn;
+            double* acc = D.dft_acc + 2 * (long long)q;
+            double* cmp = D.dft_cmp + 2 * (long long)q;
+            const double yr = tr - cmp[0], sr_ = acc[0] + yr;
+            cmp[0] = (sr_ - acc[0]) - yr;
+            acc[0] = sr_;
+            const double yi = ti - cmp[1], si = acc[1] + yi;
+            cmp[1] = (si - acc[1]) - yi;
+            acc[1] = si;
+        }
+    }
 }
 
 // 2-D video slice, ref :6833-6958 (cell-centred E, H halves at both steps)
@@ -676,7 +704,7 @@ void ff_batch_prepare() {
 }
 int launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {
     int n = 0;
-    if (D.plane_sum || D.ff_pc) {
+    if (D.plane_sum || D.ff_pc || D.ndft) {
         if (P.kmax) k_taps<cf><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
         else k_taps<float><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
         n++;

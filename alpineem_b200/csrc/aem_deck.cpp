@@ -332,6 +332,19 @@ void apply_extensions(Deck& d, const std::string& text) {
         } else if (key == "geometry_bin") {
             if (val != "yes" && val != "no") throw DeckError("extension geometry_bin must be yes or no");
             d.ext_geometry_bin = val == "yes";
+        } else if (key == "dft_freqs") {
+            // dft_freqs f_start f_stop count: count frequencies spaced evenly
+            // from f_start to f_stop inclusive (Hz)
+            std::string v1, v2;
+            char *e0 = nullptr, *e1 = nullptr, *e2 = nullptr;
+            if (!(ls >> v1 >> v2)) throw DeckError("extension dft_freqs needs f_start f_stop count");
+            const double f0 = std::strtod(val.c_str(), &e0), f1 = std::strtod(v1.c_str(), &e1);
+            const long n = std::strtol(v2.c_str(), &e2, 10);
+            if (*e0 || *e1 || *e2 || !(f0 >= 0.0) || !(f1 >= f0) || n < 1 || n > AEM_MAX_DFT_FREQS)
+                throw DeckError("extension dft_freqs needs 0 <= f_start <= f_stop and 1 <= count <= " +
+                                std::to_string(AEM_MAX_DFT_FREQS));
+            d.ext_dft_freqs.resize((size_t)n);
+            for (long q = 0; q < n; q++) d.ext_dft_freqs[q] = n == 1 ? f0 : f0 + (f1 - f0) * (double)q / (double)(n - 1);
         } else {
             throw DeckError("unknown extension '" + key + "'");
         }

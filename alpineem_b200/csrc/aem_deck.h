@@ -111,6 +111,7 @@ struct Deck {
     //   geometry_bin no  do not build or write <name>_geometry.bin
     int ext_pml_cells = 0;
     bool ext_geometry_bin = true;
+    std::vector<double> ext_dft_freqs;  // on-the-fly spectra of the per-step series (Hz)
 };
 
 // Parse an inputs.txt.  `kmax` selects the constant-k periodic grammar

@@ -80,6 +80,14 @@ struct TapDev {
     int video;                  // 2-D slice export
     int slice_dir, slice_loc, v1, v2;
     void* vid[6];               // Ex,Hx,Ey,Hy,Ez,Hz each (v1, v2, steps)
+    // on-the-fly spectra: X[s][f] += x_s[m] exp(-i 2 pi f m dt) every step
+    // (m = step - 1), FP64 sums with Kahan compensation
+    int ndft, nser;             // frequencies, series
+    double dft_dt;
+    const double* dft_f;        // [ndft] Hz
+    double* dft_acc;            // [nser][ndft][re, im]
+    double* dft_cmp;            // compensations, same layout
+    const void* ser[AEM_MAX_DFT_SERIES];  // per-step samples of each series
 };
 
 int launch_update_h(const AemParams& P, int counter, cudaStream_t s);

@@ -589,6 +589,49 @@ void Solver::setup_taps() {
         T.v2 = d.vid2;
         for (int q = 0; q < 6; q++) T.vid[q] = alloc((size_t)T.v1 * T.v2 * d.steps * es_);
     }
+    dft_series_.clear();
+    if (!d.ext_dft_freqs.empty()) {
+        // series in the order of the probe kinds: plane sums, then port voltages
+        auto add = [&](int kind, int index, const void* p) {
+            T.ser[dft_series_.size()] = p;
+            dft_series_.push_back({kind, index});
+        };
+        if (T.plane_sum) {
+            add(1, 0, T.refl);
+            add(2, 0, T.trans);
+            if (d.kmax) { add(3, 0, T.refl_tm); add(4, 0, T.trans_tm); }
+        }
+        for (int q = 0; q < PS_.n; q++) add(5, q, PS_.p[q].vout);
+        if (dft_series_.empty())
+            throw DeckError("extension dft_freqs: the deck records no per-step series (unit-cell plane sums or ports)");
+        T.nser = (int)dft_series_.size();
+        T.ndft = (int)d.ext_dft_freqs.size();
+        T.dft_dt = (double)d.del_t;
+        T.dft_f = (const double*)upload(d.ext_dft_freqs);
+        T.dft_acc = (double*)alloc((size_t)T.nser * T.ndft * 2 * sizeof(double));
+        T.dft_cmp = (double*)alloc((size_t)T.nser * T.ndft * 2 * sizeof(double));
+    }
+}
+
+// spectrum of one per-step series over the steps run so far
+int Solver::read_spectrum(int kind, int index, int n, double* freqs, double* re, double* im) {
+    int sr = -1;
+    for (size_t q = 0; q < dft_series_.size(); q++)
+        if (dft_series_[q].first == kind && dft_series_[q].second == index) sr = (int)q;
+    if (!TP_.ndft) throw std::invalid_argument("no on-the-fly spectra: the run has no dft_freqs extension");
+    if (sr < 0) throw std::invalid_argument("no spectrum of that series (kind 1..4 plane sums, 5 port voltage)");
+    const int nf = std::min(n, TP_.ndft);
+    std::vector<double> buf((size_t)TP_.ndft * 2);
+    AEM_CUDA(cudaMemcpyAsync(buf.data(), TP_.dft_acc + (size_t)sr * TP_.ndft * 2, buf.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream_));
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    d2h_bytes_ += buf.size() * sizeof(double);
+    for (int f = 0; f < nf; f++) {
+        if (freqs) freqs[f] = m_.d.ext_dft_freqs[f];
+        re[f] = buf[2 * f];
+        if (im) im[f] = buf[2 * f + 1];
+    }
+    return nf;
 }
 
 // Full-field export files, opened at setup like the reference's units
@@ -708,11 +751,12 @@ void Solver::read_probe(int kind, int index, int first, int n, double* re, doubl
     if (kind == 5) {
         if (index < 0 || index >= PS_.n) throw std::invalid_argument("no such port");
         src = PS_.p[index].vout;
-    } else if (kind == 1 || kind == 2) {
+    } else if (kind >= 1 && kind <= 4) {
         if (!TP_.plane_sum) throw std::invalid_argument("the deck has no reflection/transmission planes");
-        src = kind == 1 ? TP_.refl : TP_.trans;
+        if (kind >= 3 && !m_.d.kmax) throw std::invalid_argument("TM plane sums (kinds 3, 4) exist in kmax runs only");
+        src = kind == 1 ? TP_.refl : kind == 2 ? TP_.trans : kind == 3 ? TP_.refl_tm : TP_.trans_tm;
     } else {
-        throw std::invalid_argument("probe kind must be 1, 2 or 5");
+        throw std::invalid_argument("probe kind must be 1..5");
     }
     if (first < 1 || n < 0 || first - 1 + n > done_) throw std::invalid_argument("steps outside those run so far");
     std::vector<char> buf((size_t)n * es_);

@@ -76,6 +76,7 @@ class Solver {
     // raw per-step samples on the device: port voltage (kind 5, Voltage_out)
     // or unnormalised plane sums (kind 1 reflected, 2 transmitted)
     void read_probe(int kind, int index, int first, int n, double* re, double* im);
+    int read_spectrum(int kind, int index, int n, double* freqs, double* re, double* im);
     // bytes the fused Yee/CPML update must move per step (algorithmic)
     double algorithmic_bytes_per_step() const;
     // Huygens-surface cells (both planes of each axis) and far-field angles
@@ -135,6 +136,7 @@ class Solver {
     // far-field angle whose bins angle q copies (q itself unless q is a
     // second angle of the same direction, e.g. a pole at another phi)
     std::vector<int> ff_canon_;
+    std::vector<std::pair<int, int>> dft_series_;  // (probe kind, index) of each on-the-fly spectrum
     long long launches_ = 0;
     size_t h2d_bytes_ = 0, d2h_bytes_ = 0;
     struct ProfMark {

@@ -25,6 +25,8 @@
 #define AEM_MAX_SHEET_PLANES 16
 #define AEM_MAX_PORTS 16
 #define AEM_MAX_FF_ANGLES 4096
+#define AEM_MAX_DFT_FREQS 4096
+#define AEM_MAX_DFT_SERIES (4 + AEM_MAX_PORTS)
 
 // Per-material constants (cell properties), ref materials_properties(:,:,:)
 struct AemMaterial {

@@ -66,6 +66,11 @@ def dipole_ellipsoids(n=1024, steps=4000, n_ell=64, seed=2, pml_cells=16, dl="2E
     return d, ext, bulk
 
 
+# sidecar extension of every kmax_batch instance: on-the-fly spectra of the
+# TE/TM reflected and transmitted plane sums at 128 frequencies
+KMAX_BATCH_EXT = "dft_freqs 2e9 1.8e10 128\n"
+
+
 def kmax_batch(n_inst=64, steps=6000, seed=3, dl="1E-3", f="10E9", nxy=64, depth=10, patch=16):
     """Batched constant-k unit cells (the fan-out that
     utility_scripts/parallel_kmax.py runs as separate processes): n_inst decks

@@ -201,24 +201,31 @@ def reference_arm(args):
 
 
 def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
-    from alpineem_b200.parallel import shard
-    """The batched constant-k sweep (64 unit cells, workloads.kmax_batch):
-    wall time of the instances run one after another with plain launches,
-    against the same instances advanced together by aem_run_batch (one
-    stream per instance, one CUDA graph of g steps per instance).  Ranks
-    take every world-th instance.  Setup, a 4-step warm-up of each run and
-    the graph capture (one untimed chunk) are outside both timings."""
+    """The batched constant-k sweep (64 unit cells, workloads.kmax_batch,
+    each with on-the-fly spectra of its four plane sums at 128 frequencies,
+    workloads.KMAX_BATCH_EXT): wall time of the instances run one after
+    another with plain launches, against the same instances advanced
+    together by aem_run_batch (one stream per instance, one CUDA graph of g
+    steps per instance).  Ranks take every world-th instance.  Setup, a
+    4-step warm-up of each run and the graph capture (one untimed chunk) are
+    outside both timings."""
+    import numpy as np
+
     import alpineem_b200 as ab
+    from alpineem_b200.parallel import shard
     from alpineem_b200 import workloads
     from alpineem_b200.deck import deck_text
 
     warm = 4
+    ext = workloads.KMAX_BATCH_EXT
+    kinds = ("reflected", "transmitted", "reflected_tm", "transmitted_tm")
     decks = shard(workloads.kmax_batch(steps=warm + 2 * g + steps), rank, world)
     tmp = tempfile.mkdtemp(prefix="aem_batch_")
     seq = 0.0
     cells = 0
+    spectra = []
     for d in decks:
-        sim = ab.Simulation(deck_text=deck_text(d), kmax=True, outdir=tmp)
+        sim = ab.Simulation(deck_text=deck_text(d), ext_text=ext, kmax=True, outdir=tmp)
         cells += sim.workload[0]
         sim.run(warm + g)
         sim.synchronize()
@@ -226,8 +233,9 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
         sim.run(steps)
         sim.synchronize()
         seq += time.perf_counter() - t0
+        spectra.append([sim.spectrum(k)[1] for k in kinds])
         sim.close()
-    sims = [ab.Simulation(deck_text=deck_text(d), kmax=True, outdir=tmp) for d in decks]
+    sims = [ab.Simulation(deck_text=deck_text(d), ext_text=ext, kmax=True, outdir=tmp) for d in decks]
     try:
         for s in sims:
             s.run(warm)
@@ -240,6 +248,8 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
         for s in sims:
             s.synchronize()
         bat = time.perf_counter() - t0
+        # the same steps in the same order: the spectra must agree bit for bit
+        same = all(np.array_equal(a, b) for s, ref in zip(sims, spectra) for a, b in zip([s.spectrum(k)[1] for k in kinds], ref))
     finally:
         for s in sims:
             s.close()
@@ -247,7 +257,9 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
     return {"workload": "kmax_batch", "instances": 64, "grid": "64 x 64 x Z, Z in {128..512}, complex64",
             "steps_timed": steps, "steps_per_graph": g, "sequential_s": round(seq, 4), "batched_s": round(bat, 4),
             "speedup": round(seq / bat, 2),
-            "batched_mcell_updates_per_s": round(world * cells * steps / bat / 1e6, 1)}
+            "batched_mcell_updates_per_s": round(world * cells * steps / bat / 1e6, 1),
+            "spectra": "128 frequencies x 4 plane sums per instance, FP64 Kahan, accumulated every step",
+            "spectra_equal_sequential_batched": bool(same)}
 
 
 def adjoint_gradient(args, max_over_ranks):

@@ -92,9 +92,26 @@ int aem_run_batch(aem_handle* const* handles, int count, int nsteps, int steps_p
 /* Raw per-step samples of the steps run so far, before the normalisation
  * that aem_write_outputs applies: kind 5 = voltage of port `index`
  * (Voltage_out, fdtd_solver.f90:8241-8243), kind 1 / 2 = reflected /
- * transmitted plane sums (:7005-7103).  Steps first_step .. first_step+n-1
+ * transmitted plane sums (:7005-7103; TE for kmax), kind 3 / 4 = their
+ * kmax TM sums (:7105-7190).  Steps first_step .. first_step+n-1
  * (1-based); im may be NULL.  Synchronises the handle's stream. */
 int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, double* re, double* im);
+
+/* On-the-fly spectrum of a per-step series (the run's sidecar extension
+ * `dft_freqs f_start f_stop count`): X(f) = sum over the steps run so far of
+ * x[m] exp(-i 2 pi f m dt), m = step - 1, dt the time step, accumulated in
+ * FP64 with Kahan compensation by the per-step tap kernel.  kind / index as
+ * aem_read_probe (1 / 2 reflected / transmitted plane sums, TE for kmax;
+ * 3 / 4 their TM sums (kmax); 5 port `index`), on the raw samples.  Copies
+ * min(n, count) values; freqs (Hz) and im may be NULL.  Returns the number
+ * copied, or a negative error code.  Synchronises the handle's stream.
+ * Replaces the post-hoc FFT of utility_scripts/post_processor*.py for these
+ * series. */
+int aem_read_spectrum(aem_handle* h, int kind, int index, int n, double* freqs, double* re, double* im);
+
+/* The run's time step del_t in seconds (fdtd_solver.f90:1312, FP32
+ * value widened). */
+int aem_time_step(aem_handle* h, double* dt);
 
 /* Phases of a time step, for per-phase device timing. */
 #define AEM_NPHASE 8

@@ -61,3 +61,8 @@ def test_check_deck_reference_errors(tmp_path):
         ab.check_deck(base, "no_such_key 3\n")
     with pytest.raises(ab.AemError, match="pml_cells"):
         ab.check_deck(base, "pml_cells -2\n")
+    for ext in ("dft_freqs 1e9\n", "dft_freqs 2e9 1e9 8\n", "dft_freqs 1e9 2e9 0\n", "dft_freqs -1 2e9 8\n",
+                "dft_freqs 1e9 2e9 x\n", "dft_freqs 1e9 2e9 5000\n"):
+        with pytest.raises(ab.AemError, match="dft_freqs"):
+            ab.check_deck(base, ext)
+    assert ab.check_deck(base, "dft_freqs 1e9 2e10 128\n") == ab.check_deck(base)
