@@ -399,6 +399,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : 2) k_upd
             id0 = C[c]; idx = C[cxm]; idy = C[cym]; idz = C[czm];
             idxy = C[lin(P, pxd, pyd, pz)]; idxz = C[lin(P, pxd, py, pzd)]; idyz = C[lin(P, px, pyd, pzd)];
         }
+        // a sheet plane through this position (both sheet loops below act
+        // only there)
+        bool sheet_here = false;
+        for (int s = 0; s < P.nsheet; s++) {
+            const AemSheetPlane& S = P.sheet[s];
+            sheet_here |= (S.axis == 0 ? px : S.axis == 1 ? py : pz) == S.pos;
+        }
 
 #pragma unroll
         for (int comp = 0; comp < 3; comp++) {
@@ -420,14 +427,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : 2) k_upd
             }
             const T curl = d1 * den1 + d2 * den2;
             float ga = co.ga, gb = co.gb;
-            if (P.nsheet) sheet_override(P, comp, px, py, pz, &ga, &gb);
+            if (sheet_here) sheet_override(P, comp, px, py, pz, &ga, &gb);
             const T eold = comp == 0 ? eo0 : comp == 1 ? eo1 : eo2;
             T e = eold;
             if (P.cpml_split != 2) {
             e = ga * eold + gb * curl;
 
             // sheet sub-cell field of the normal component, ref :5714-5780
-            for (int s = 0; s < P.nsheet; s++) {
+            for (int s = 0; sheet_here && s < P.nsheet; s++) {
                 const AemSheetPlane& S = P.sheet[s];
                 if (S.axis != comp) continue;
                 const int pn = comp == 0 ? px : comp == 1 ? py : pz;
