@@ -68,6 +68,8 @@ def load_library():
     lib.aem_read_probe.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.aem_time_step.argtypes = [h, ctypes.POINTER(ctypes.c_double)]
+    lib.aem_checkpoint_save.argtypes = [h, ctypes.c_char_p]
+    lib.aem_checkpoint_load.argtypes = [h, ctypes.c_char_p]
     lib.aem_read_spectrum.argtypes = [h, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.aem_profile.argtypes = [h, ctypes.c_int]
@@ -263,6 +265,15 @@ class Simulation:
         re, im = np.zeros(n), np.zeros(n)
         self._check(self._lib.aem_read_probe(self._h, k, int(index), int(first), int(n), _dptr(re), _dptr(im)))
         return (re + 1j * im) if self.kmax else re
+
+    def checkpoint_save(self, path):
+        """Write the whole run state after the steps done so far to `path`."""
+        self._check(self._lib.aem_checkpoint_save(self._h, os.fsencode(path)))
+
+    def checkpoint_load(self, path):
+        """Restore a state written by checkpoint_save of a run of the same
+        deck; the run continues from that step."""
+        self._check(self._lib.aem_checkpoint_load(self._h, os.fsencode(path)))
 
     def spectrum(self, kind, index=0, n=4096):
         """On-the-fly spectrum of a per-step series over the steps run so

@@ -267,6 +267,22 @@ int aem_read_spectrum(aem_handle* h, int kind, int index, int n, double* freqs, 
     return guarded(h, [&]() { return h->s->read_spectrum(kind, index, n, freqs, re, im); });
 }
 
+int aem_checkpoint_save(aem_handle* h, const char* path) {
+    if (!h || !path) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->checkpoint_save(path);
+        return AEM_OK;
+    });
+}
+
+int aem_checkpoint_load(aem_handle* h, const char* path) {
+    if (!h || !path) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->checkpoint_load(path);
+        return AEM_OK;
+    });
+}
+
 int aem_time_step(aem_handle* h, double* dt) {
     if (!h || !dt) return fail(h, AEM_ERR_ARG, "bad argument");
     *dt = (double)h->s->model().d.del_t;

@@ -47,6 +47,7 @@ void* Solver::alloc(size_t bytes) {
     }
     AEM_CUDA(cudaMemsetAsync(p, 0, bytes, stream_));
     bufs_.push_back(p);
+    buf_bytes_.push_back(bytes);
     dev_bytes_ += bytes;
     return p;
 }
@@ -87,6 +88,7 @@ void Solver::init() {
         setup_full();
         setup_fused();
         AEM_CUDA(cudaStreamSynchronize(stream_));
+        nstate_ = bufs_.size();
     } catch (...) {
         release();  // a throwing constructor runs no destructor
         throw;
@@ -153,6 +155,7 @@ void Solver::release() {
     release_graph();
     for (void* p : bufs_) cudaFree(p);
     bufs_.clear();
+    buf_bytes_.clear();
     for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
     prof_pool_.clear();
     if (stream_) cudaStreamDestroy(stream_);
@@ -897,6 +900,101 @@ void Solver::capture_graph(int g) {
 void Solver::run_graph(int n, int g) {
     Solver* self = this;
     run_batch(&self, 1, n, g);
+}
+
+// Checkpoint file: "AEMCKPT1", then int64 fields (kmax, cells, steps,
+// done, far-field batch start, buffer count), the byte size of every
+// setup-time device buffer, then the buffers' bytes in allocation order.
+// The buffers hold the fields, CPML psi, port lines, far-field bins and
+// difference buffers, per-step taps and spectra, and the constant tables;
+// a handle made from the same deck allocates the same buffers in the same
+// order and sizes, which the load checks.  On the fused path the field
+// buffers swap every step, so the loading handle swaps its pointers when
+// its step count and the snapshot's differ in parity.
+namespace {
+constexpr char CKPT_MAGIC[8] = {'A', 'E', 'M', 'C', 'K', 'P', 'T', '1'};
+constexpr size_t CKPT_CHUNK = 64u << 20;
+}  // namespace
+
+void Solver::checkpoint_save(const std::string& path) {
+    if (full_.f[0]) throw std::invalid_argument("checkpoints are not supported while the full-field export is on");
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::invalid_argument("cannot write checkpoint '" + path + "'");
+    void* stage = nullptr;
+    bool ok = true;
+    try {
+        AEM_CUDA(cudaMallocHost(&stage, CKPT_CHUNK));
+        const long long hdr[6] = {m_.d.kmax ? 1 : 0, (long long)m_.cells, m_.d.steps, done_, ff_n0_, (long long)nstate_};
+        ok = std::fwrite(CKPT_MAGIC, 1, 8, f) == 8 && std::fwrite(hdr, sizeof hdr, 1, f) == 1;
+        for (size_t b = 0; ok && b < nstate_; b++) {
+            const long long n = (long long)buf_bytes_[b];
+            ok = std::fwrite(&n, sizeof n, 1, f) == 1;
+        }
+        for (size_t b = 0; ok && b < nstate_; b++)
+            for (size_t o = 0; ok && o < buf_bytes_[b]; o += CKPT_CHUNK) {
+                const size_t n = std::min(CKPT_CHUNK, buf_bytes_[b] - o);
+                AEM_CUDA(cudaMemcpyAsync(stage, (const char*)bufs_[b] + o, n, cudaMemcpyDeviceToHost, stream_));
+                AEM_CUDA(cudaStreamSynchronize(stream_));
+                ok = std::fwrite(stage, 1, n, f) == n;
+                d2h_bytes_ += n;
+            }
+    } catch (...) {
+        if (stage) cudaFreeHost(stage);
+        std::fclose(f);
+        throw;
+    }
+    cudaFreeHost(stage);
+    if (std::fclose(f) != 0) ok = false;
+    if (!ok) throw std::runtime_error("writing checkpoint '" + path + "' failed");
+}
+
+void Solver::checkpoint_load(const std::string& path) {
+    if (full_.f[0]) throw std::invalid_argument("checkpoints are not supported while the full-field export is on");
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::invalid_argument("cannot open checkpoint '" + path + "'");
+    void* stage = nullptr;
+    long long hdr[6] = {0, 0, 0, 0, 0, 0};
+    try {
+        char magic[8];
+        if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, CKPT_MAGIC, 8) != 0 || std::fread(hdr, sizeof hdr, 1, f) != 1)
+            throw std::invalid_argument("'" + path + "' is not a checkpoint file");
+        bool match = hdr[0] == (m_.d.kmax ? 1 : 0) && hdr[1] == (long long)m_.cells && hdr[2] == m_.d.steps &&
+                     hdr[5] == (long long)nstate_ && hdr[3] >= 0 && hdr[3] <= m_.d.steps;
+        for (size_t b = 0; match && b < nstate_; b++) {
+            long long n = 0;
+            if (std::fread(&n, sizeof n, 1, f) != 1) throw std::invalid_argument("checkpoint '" + path + "' is truncated");
+            match = n == (long long)buf_bytes_[b];
+        }
+        if (!match) throw std::invalid_argument("checkpoint '" + path + "' was not written by a run of this deck");
+        AEM_CUDA(cudaStreamSynchronize(stream_));
+        release_graph();
+        AEM_CUDA(cudaMallocHost(&stage, CKPT_CHUNK));
+        for (size_t b = 0; b < nstate_; b++)
+            for (size_t o = 0; o < buf_bytes_[b]; o += CKPT_CHUNK) {
+                const size_t n = std::min(CKPT_CHUNK, buf_bytes_[b] - o);
+                if (std::fread(stage, 1, n, f) != n) throw std::invalid_argument("checkpoint '" + path + "' is truncated");
+                AEM_CUDA(cudaMemcpyAsync((char*)bufs_[b] + o, stage, n, cudaMemcpyHostToDevice, stream_));
+                AEM_CUDA(cudaStreamSynchronize(stream_));
+                h2d_bytes_ += n;
+            }
+    } catch (...) {
+        if (stage) cudaFreeHost(stage);
+        std::fclose(f);
+        throw;
+    }
+    cudaFreeHost(stage);
+    std::fclose(f);
+    if (fused_ && ((done_ ^ (int)hdr[3]) & 1)) {  // the same pointer swaps as one step()
+        for (int c = 0; c < 3; c++) {
+            std::swap(P_.E[c], P_.E2[c]);
+            std::swap(P_.H[c], P_.H2[c]);
+            for (int a = 0; a < 3; a++)
+                for (int s = 0; s < 2; s++) std::swap(P_.psi_h[c][a][s], P_.psi_h2[c][a][s]);
+        }
+    }
+    done_ = (int)hdr[3];
+    ff_n0_ = (int)hdr[4];
 }
 
 void Solver::run_batch(Solver* const* s, int count, int n, int g) {

@@ -40,6 +40,10 @@ class Solver {
     // run eagerly.  Graph chunks need g even on the fused path (the field
     // buffers swap each step) and g a multiple of the far-field batch.
     void run_graph(int n, int g);
+    // whole-run snapshot (device buffers of the setup, step counters) to a
+    // file, and its restore into a handle made from the same deck
+    void checkpoint_save(const std::string& path);
+    void checkpoint_load(const std::string& path);
     // the launch part of run_graph for a batch of solvers on their own
     // streams: every solver gets to the same point, then the chunks of all
     // solvers are launched round-robin so that their graphs overlap
@@ -126,6 +130,8 @@ class Solver {
     FarFieldDev FF_{};
     TapDev TP_{};
     std::vector<void*> bufs_;
+    std::vector<size_t> buf_bytes_;  // size of each buffer of bufs_
+    size_t nstate_ = 0;              // buffers allocated by init(): the run's device state
     size_t dev_bytes_ = 0;
     int es_ = 4;  // bytes per field value
     int done_ = 0;

@@ -109,6 +109,19 @@ int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, do
  * series. */
 int aem_read_spectrum(aem_handle* h, int kind, int index, int n, double* freqs, double* re, double* im);
 
+/* Checkpoint / resume (no reference counterpart: the reference restarts a
+ * run from step 1).  aem_checkpoint_save writes the whole run state after
+ * the steps done so far to a file: every device buffer the handle set up
+ * (fields, CPML psi, port lines, far-field bins and difference buffer,
+ * per-step taps and spectra, tables) and the step counters.
+ * aem_checkpoint_load restores it into a handle created from the same deck
+ * (and extensions), at any step count; the run then continues as if it had
+ * never stopped (fields bit-identical to an uninterrupted run).  A file from
+ * another deck is rejected with AEM_ERR_ARG.  Not available while the
+ * full-field export is on.  Both synchronise the handle's stream. */
+int aem_checkpoint_save(aem_handle* h, const char* path);
+int aem_checkpoint_load(aem_handle* h, const char* path);
+
 /* The run's time step del_t in seconds (fdtd_solver.f90:1312, FP32
  * value widened). */
 int aem_time_step(aem_handle* h, double* dt);
