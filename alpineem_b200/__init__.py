@@ -36,6 +36,11 @@ class AemError(RuntimeError):
     """A failing call of the solver library (message from aem_last_error)."""
 
 
+class AemDiverged(AemError):
+    """A run stopped by the watchdog (extension `watchdog K`): E or H holds a
+    NaN or Inf."""
+
+
 def load_library():
     """Load libalpineem_b200.so (built in-tree by alpineem_b200/build.py)."""
     global _lib
@@ -185,6 +190,8 @@ class Simulation:
         self.kmax = kmax
 
     def _check(self, rc):
+        if rc == -5:
+            raise AemDiverged(self._lib.aem_last_error(self._h).decode())
         if rc < 0:
             raise AemError(self._lib.aem_last_error(self._h).decode())
         return rc

@@ -34,6 +34,8 @@ int guarded(aem_handle* h, F&& f) {
         return f();
     } catch (const aem::DeckError& e) {
         return fail(h, AEM_ERR_INPUT, e.what());
+    } catch (const aem::Diverged& e) {
+        return fail(h, AEM_ERR_DIVERGED, e.what());
     } catch (const std::invalid_argument& e) {
         return fail(h, AEM_ERR_ARG, e.what());
     } catch (const std::runtime_error& e) {

@@ -599,6 +599,27 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
     }
 }
 
+// watchdog: flag a non-finite value (exponent bits all set) in any of the
+// six field arrays, read as float4 (n4 float4 per array)
+__global__ void k_nonfinite(const __grid_constant__ FieldPtrs F, long long n4, int* flag) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (int a = 0; a < 6; a++) {
+        const uint4* p = reinterpret_cast<const uint4*>(F.p[a]);
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const uint4 v = __ldg(p + i);
+            bad |= ((v.x & 0x7f800000u) == 0x7f800000u) | ((v.y & 0x7f800000u) == 0x7f800000u) |
+                   ((v.z & 0x7f800000u) == 0x7f800000u) | ((v.w & 0x7f800000u) == 0x7f800000u);
+        }
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
+}
+
+int launch_nonfinite(const FieldPtrs& F, long long n4, int* flag, cudaStream_t s) {
+    k_nonfinite<<<148 * 4, 256, 0, s>>>(F, n4, flag);
+    return 1;
+}
+
 // 2-D video slice, ref :6833-6958 (cell-centred E, H halves at both steps)
 template <typename T>
 __global__ void k_video(const __grid_constant__ AemParams P, const __grid_constant__ TapDev D, int counter, int steps) {

@@ -332,6 +332,13 @@ void apply_extensions(Deck& d, const std::string& text) {
         } else if (key == "geometry_bin") {
             if (val != "yes" && val != "no") throw DeckError("extension geometry_bin must be yes or no");
             d.ext_geometry_bin = val == "yes";
+        } else if (key == "watchdog") {
+            // watchdog K: every K steps, stop the run if E or H holds a
+            // non-finite value
+            char* end = nullptr;
+            long v = std::strtol(val.c_str(), &end, 10);
+            if (*end || v < 0 || v > 1000000000L) throw DeckError("extension watchdog must be a step count >= 0");
+            d.ext_watchdog = (int)v;
         } else if (key == "dft_freqs") {
             // dft_freqs f_start f_stop count: count frequencies spaced evenly
             // from f_start to f_stop inclusive (Hz)

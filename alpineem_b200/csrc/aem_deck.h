@@ -14,6 +14,11 @@ struct DeckError : std::runtime_error {
     explicit DeckError(const std::string& m) : std::runtime_error(m) {}
 };
 
+// a run stopped by the watchdog: a non-finite field value
+struct Diverged : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 struct VolumeMaterial {
     float id = 0;
     float eps[3] = {1, 1, 1};
@@ -112,6 +117,7 @@ struct Deck {
     int ext_pml_cells = 0;
     bool ext_geometry_bin = true;
     std::vector<double> ext_dft_freqs;  // on-the-fly spectra of the per-step series (Hz)
+    int ext_watchdog = 0;               // steps between non-finite field checks (0: off)
 };
 
 // Parse an inputs.txt.  `kmax` selects the constant-k periodic grammar

@@ -90,6 +90,12 @@ struct TapDev {
     const void* ser[AEM_MAX_DFT_SERIES];  // per-step samples of each series
 };
 
+// the six field arrays (Ex, Ey, Ez, Hx, Hy, Hz) the watchdog scans
+struct FieldPtrs {
+    const void* p[6];
+};
+int launch_nonfinite(const FieldPtrs& F, long long n4, int* flag, cudaStream_t s);  // *flag = 1 on a NaN or Inf
+
 int launch_update_h(const AemParams& P, int counter, cudaStream_t s);
 int launch_update_e(const AemParams& P, int counter, cudaStream_t s);
 int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);

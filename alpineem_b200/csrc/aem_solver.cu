@@ -39,6 +39,13 @@ static std::string dir_of(const std::string& p) {
 void* Solver::alloc(size_t bytes) {
     void* p = nullptr;
     if (bytes == 0) bytes = 16;
+    // fault injection: AEM_FAIL_ALLOC_AT=n fails the n-th allocation of this
+    // handle as if the device were out of memory (host-side; tests the
+    // error path and the release of what was allocated before)
+    if (const char* v = std::getenv("AEM_FAIL_ALLOC_AT"))
+        if (std::atol(v) == (long)bufs_.size() + 1)
+            throw std::runtime_error("CUDA error: out of memory (injected by AEM_FAIL_ALLOC_AT) allocating " +
+                                     std::to_string(bytes) + " bytes");
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();  // do not leave the failure pending for later calls
@@ -87,6 +94,7 @@ void Solver::init() {
         setup_taps();
         setup_full();
         setup_fused();
+        if (m_.d.ext_watchdog > 0) wd_flag_ = (int*)alloc(sizeof(int));
         AEM_CUDA(cudaStreamSynchronize(stream_));
         nstate_ = bufs_.size();
     } catch (...) {
@@ -829,10 +837,25 @@ void Solver::flush_farfield(int last) {
     ff_n0_ = last + 1;
 }
 
+// every K steps (extension watchdog K): scan the current E and H for a
+// non-finite value; the run stops with Diverged at the first step found so
+void Solver::watchdog_check() {
+    FieldPtrs F;
+    for (int c = 0; c < 3; c++) { F.p[c] = P_.E[c]; F.p[3 + c] = P_.H[c]; }
+    launches_ += launch_nonfinite(F, (long long)m_.cells * es_ / 16, wd_flag_, stream_);
+    int bad = 0;
+    AEM_CUDA(cudaMemcpyAsync(&bad, wd_flag_, sizeof bad, cudaMemcpyDeviceToHost, stream_));
+    AEM_CUDA(cudaStreamSynchronize(stream_));
+    d2h_bytes_ += sizeof bad;
+    if (bad) throw Diverged("the fields diverged: a non-finite value at step " + std::to_string(done_));
+}
+
 void Solver::run(int n) {
+    const int K = m_.d.ext_watchdog;
     for (int q = 0; q < n && done_ < m_.d.steps; q++) {
         done_++;
         step(done_);
+        if (K > 0 && done_ % K == 0) watchdog_check();
     }
     // the last step bins whatever the batch buffer still holds; earlier
     // partial batches wait for more steps (or for flush())
@@ -1026,6 +1049,9 @@ void Solver::run_batch(Solver* const* s, int count, int n, int g) {
             v.launches_ += v.graph_launches_;
             if (v.FF_.tb > 1) v.ff_n0_ = v.done_ + 1;
             any = true;
+            // a chunk that passed a watchdog step is checked at its end
+            const int K = v.m_.d.ext_watchdog;
+            if (K > 0 && v.done_ / K != (v.done_ - g) / K) v.watchdog_check();
         }
     }
     // the rest eagerly (run() also bins the last far-field batch)

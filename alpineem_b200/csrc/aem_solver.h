@@ -119,6 +119,7 @@ class Solver {
     void full_flush();
     void capture_graph(int g);
     void release_graph();
+    void watchdog_check();
     template <typename Fn>
     void phase(int ph, Fn&& fn);
     cudaEvent_t prof_event();
@@ -156,6 +157,7 @@ class Solver {
     cudaStream_t stream_ = nullptr;
     // graph replay
     int* dstep_ = nullptr;          // device step counter
+    int* wd_flag_ = nullptr;        // watchdog: set by k_nonfinite
     cudaGraphExec_t graph_ = nullptr;
     // full-field export (every step's averaged fields to <name>_full_*.bin):
     // the averages go to a device staging buffer, a second stream copies

@@ -34,6 +34,7 @@ typedef struct aem_handle aem_handle;
 #define AEM_ERR_CUDA (-2)     /* CUDA runtime failure (no device, out of memory, launch error) */
 #define AEM_ERR_ARG (-3)      /* bad argument to this API */
 #define AEM_ERR_STATE (-4)    /* call out of order (e.g. write before the last step) */
+#define AEM_ERR_DIVERGED (-5) /* the fields hold a non-finite value (extension `watchdog K`, checked every K steps) */
 
 /* Deck grammar selector: the reference builds two solvers from one source
  * (fdtd_solver.f90:5-7); AEM_KMAX selects the constant-k periodic one. */

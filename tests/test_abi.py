@@ -66,3 +66,7 @@ def test_check_deck_reference_errors(tmp_path):
         with pytest.raises(ab.AemError, match="dft_freqs"):
             ab.check_deck(base, ext)
     assert ab.check_deck(base, "dft_freqs 1e9 2e10 128\n") == ab.check_deck(base)
+    for ext in ("watchdog -1\n", "watchdog x\n"):
+        with pytest.raises(ab.AemError, match="watchdog"):
+            ab.check_deck(base, ext)
+    assert ab.check_deck(base, "watchdog 100\n") == ab.check_deck(base)
