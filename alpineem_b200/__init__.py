@@ -28,6 +28,10 @@ STANDARD, KMAX = 0, 1
 SERIES = {"incident": 0, "reflected": 1, "transmitted": 2, "reflected_tm": 3, "transmitted_tm": 4,
           "port_voltage": 5, "e_theta": 6, "e_phi": 7}
 FIELDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
+# per-step samples that aem_read_probe returns; "point" is the extension
+# `probe i j k` (index 3 p + c: probe p, component c = Ex, Ey, Ez)
+PROBE_KINDS = {"reflected": 1, "transmitted": 2, "reflected_tm": 3, "transmitted_tm": 4, "port_voltage": 5,
+               "point": 6}
 
 _lib = None
 
@@ -264,9 +268,10 @@ class Simulation:
         return out + 1j * im.reshape(shape) if self.kmax else out
 
     def probe(self, kind, index=0, first=1, n=None):
-        """Raw per-step samples of the steps run so far (port voltage or
-        unnormalised plane sums); synchronises."""
-        k = SERIES[kind] if isinstance(kind, str) else int(kind)
+        """Raw per-step samples of the steps run so far (port voltage,
+        unnormalised plane sums, or a point-probe component: kind "point",
+        index 3 p + c); synchronises."""
+        k = PROBE_KINDS[kind] if isinstance(kind, str) else int(kind)
         if n is None:
             n = self.steps[0] - first + 1
         re, im = np.zeros(n), np.zeros(n)

@@ -569,6 +569,16 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
         at<T>(D.pc[3], counter - 1) = hx; at<T>(D.pc[4], counter - 1) = hy; at<T>(D.pc[5], counter - 1) = hz;
         if (counter < steps) { at<T>(D.pc[3], counter) = hx; at<T>(D.pc[4], counter) = hy; at<T>(D.pc[5], counter) = hz; }
     }
+    if (tid < 3 * D.nprobe) {
+        // point probes: cell-centred E as the phase-centre sample (ref :8273-8275)
+        const int pq = tid / 3, c = tid % 3;
+        const int i = D.prb_idx[pq][0], j = D.prb_idx[pq][1], k = D.prb_idx[pq][2];
+        T v;
+        if (c == 0) v = (fget<T>(P, P.E[0], i, j, k) + fget<T>(P, P.E[0], i, j + 1, k) + fget<T>(P, P.E[0], i, j, k + 1) + fget<T>(P, P.E[0], i, j + 1, k + 1)) / 4.0f;
+        else if (c == 1) v = (fget<T>(P, P.E[1], i, j, k) + fget<T>(P, P.E[1], i + 1, j, k) + fget<T>(P, P.E[1], i, j, k + 1) + fget<T>(P, P.E[1], i + 1, j, k + 1)) / 4.0f;
+        else v = (fget<T>(P, P.E[2], i, j, k) + fget<T>(P, P.E[2], i + 1, j, k) + fget<T>(P, P.E[2], i, j + 1, k) + fget<T>(P, P.E[2], i + 1, j + 1, k)) / 4.0f;
+        at<T>(D.prb, (long long)tid * steps + counter - 1) = v;
+    }
     if (D.ndft) {
         // this step's samples are in place (plane sums above, port voltages
         // from the E half-step's port kernel)
@@ -725,7 +735,7 @@ void ff_batch_prepare() {
 }
 int launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {
     int n = 0;
-    if (D.plane_sum || D.ff_pc || D.ndft) {
+    if (D.plane_sum || D.ff_pc || D.ndft || D.nprobe) {
         if (P.kmax) k_taps<cf><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
         else k_taps<float><<<1, 1024, 0, s>>>(P, D, F, counter, steps);
         n++;

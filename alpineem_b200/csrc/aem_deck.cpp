@@ -352,6 +352,37 @@ void apply_extensions(Deck& d, const std::string& text) {
                                 std::to_string(AEM_MAX_DFT_FREQS));
             d.ext_dft_freqs.resize((size_t)n);
             for (long q = 0; q < n; q++) d.ext_dft_freqs[q] = n == 1 ? f0 : f0 + (f1 - f0) * (double)q / (double)(n - 1);
+        } else if (key == "cpml_grading") {
+            // cpml_grading m sigma_factor kappa_max alpha_max
+            std::string v1, v2, v3;
+            char *e0 = nullptr, *e1 = nullptr, *e2 = nullptr, *e3 = nullptr;
+            if (!(ls >> v1 >> v2 >> v3)) throw DeckError("extension cpml_grading needs m sigma_factor kappa_max alpha_max");
+            const long m = std::strtol(val.c_str(), &e0, 10);
+            const float sf = std::strtof(v1.c_str(), &e1), km = std::strtof(v2.c_str(), &e2), am = std::strtof(v3.c_str(), &e3);
+            if (*e0 || *e1 || *e2 || *e3 || m < 1 || m > 8 || !(sf >= 0.0f) || !(km >= 1.0f) || !(am >= 0.0f))
+                throw DeckError("extension cpml_grading needs 1 <= m <= 8, sigma_factor >= 0, kappa_max >= 1, alpha_max >= 0");
+            d.ext_cpml = true;
+            d.ext_cpml_m = (int)m;
+            d.ext_cpml_sigma = sf;
+            d.ext_cpml_kappa = km;
+            d.ext_cpml_alpha = am;
+        } else if (key == "tfsf_inset") {
+            char* end = nullptr;
+            long v = std::strtol(val.c_str(), &end, 10);
+            if (*end || v < 2 || v > 1000000L) throw DeckError("extension tfsf_inset must be a cell index >= 2");
+            d.ext_tfsf_inset = (int)v;
+        } else if (key == "probe") {
+            // probe i j k: reference cell indices, 1 <= i <= nx - 1 (the
+            // cell-centred average reads i and i+1)
+            std::string v1, v2;
+            char *e0 = nullptr, *e1 = nullptr, *e2 = nullptr;
+            if (!(ls >> v1 >> v2)) throw DeckError("extension probe needs i j k");
+            const long i = std::strtol(val.c_str(), &e0, 10), j = std::strtol(v1.c_str(), &e1, 10),
+                       k = std::strtol(v2.c_str(), &e2, 10);
+            if (*e0 || *e1 || *e2 || i < 1 || j < 1 || k < 1) throw DeckError("extension probe needs cell indices >= 1");
+            if ((int)d.ext_probes.size() >= AEM_MAX_PROBES)
+                throw DeckError("extension probe: at most " + std::to_string(AEM_MAX_PROBES) + " probes");
+            d.ext_probes.push_back({(int)i, (int)j, (int)k});
         } else {
             throw DeckError("unknown extension '" + key + "'");
         }
@@ -389,6 +420,15 @@ void derive(Deck& d) {
         d.lo[a] = 1;
         d.hi[a] = N[a] - 1;
         if (!d.pbc[a]) { d.lo[a] = d.npml[a][0] + 3; d.hi[a] = N[a] - d.npml[a][1] - 3; }
+        // extension tfsf_inset: the TF/SF planes (and the far-field box
+        // derived from them) at index N and X - N instead of npml + 3
+        if (!d.pbc[a] && d.ext_tfsf_inset > 0) {
+            if (d.ext_tfsf_inset <= d.npml[a][0] || N[a] - d.ext_tfsf_inset >= N[a] - d.npml[a][1] ||
+                N[a] - d.ext_tfsf_inset <= d.ext_tfsf_inset)
+                throw DeckError("extension tfsf_inset: the TF/SF box must lie between the CPML slabs");
+            d.lo[a] = d.ext_tfsf_inset;
+            d.hi[a] = N[a] - d.ext_tfsf_inset;
+        }
     }
     if (d.is_mirror) {  // ref :1402-1447
         int a = (d.mirror_type - 1) / 2;
@@ -458,6 +498,14 @@ void derive(Deck& d) {
     if (!d.kmax) d.alpha_max = 0.03f;
     else d.alpha_max = 0.03f + 0.9f * (std::sqrt(d.kc[1] * d.kc[1] + d.kc[2] * d.kc[2] + d.kc[0] * d.kc[0])) / 377.0f;
     d.kappa_max = 7.0f;
+    d.cpml_m = 3;
+    if (d.ext_cpml) {
+        // extension cpml_grading: sigma_max = sigma_factor (m+1) / (eta0 d)
+        d.cpml_m = d.ext_cpml_m;
+        for (int a = 0; a < 3; a++) d.sig_max[a] = d.ext_cpml_sigma * ((float)(d.cpml_m + 1) / (dl[a] * eta));
+        d.alpha_max = d.ext_cpml_alpha;
+        d.kappa_max = d.ext_cpml_kappa;
+    }
     // pulse, ref :1710-1725
     if (!d.kmax) {
         d.spread = 1.0f / (2.0f * pi * d.f_center);

@@ -5,6 +5,7 @@
 // main_fdtd/master.py:51-296).  Derived quantities: :1305-1812.
 #pragma once
 #include <stdexcept>
+#include <array>
 #include <string>
 #include <vector>
 
@@ -118,6 +119,17 @@ struct Deck {
     bool ext_geometry_bin = true;
     std::vector<double> ext_dft_freqs;  // on-the-fly spectra of the per-step series (Hz)
     int ext_watchdog = 0;               // steps between non-finite field checks (0: off)
+    //   cpml_grading m sigma_factor kappa_max alpha_max   CPML profile:
+    //       polynomial order m, sigma_max = sigma_factor (m+1) / (eta0 d),
+    //       kappa and alpha maxima (absent: the reference's fixed profile)
+    //   tfsf_inset N     TF/SF planes at index N and X-N (reference: npml+3)
+    //   probe i j k      cell-centred Ex, Ey, Ez at cell (i, j, k) every step
+    bool ext_cpml = false;
+    int ext_cpml_m = 3;
+    float ext_cpml_sigma = 0, ext_cpml_kappa = 1, ext_cpml_alpha = 0;
+    int ext_tfsf_inset = 0;
+    std::vector<std::array<int, 3>> ext_probes;
+    int cpml_m = 3;                     // grading order used by the CPML tables
 };
 
 // Parse an inputs.txt.  `kmax` selects the constant-k periodic grammar

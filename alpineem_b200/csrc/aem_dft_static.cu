@@ -15,7 +15,11 @@
 // Host code cannot pass `g_dft_scratch` to a kernel by name: on the host
 // the name denotes a stand-in object, not a device address.  The device
 // address is looked up with cudaGetSymbolAddress once per device, on the
-// first call made while that device is current, and cached.
+// first call made while that device is current, and cached for the life of
+// the process.  The cache assumes the device's primary context lives that
+// long: after cudaDeviceReset (or any teardown of the primary context) the
+// array may sit at another address, so a process that resets a device must
+// not call aem_dft_static on it again.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -332,6 +332,26 @@ void Solver::finalize_and_write() {
     }
     std::fclose(f);
 
+    // point probes (extension `probe i j k`): <name>_probes.dat, a header
+    // line per probe component followed by its T samples, in the .dat
+    // file's number format; the reference has no point probes
+    if (TP_.nprobe > 0) {
+        std::vector<cplx> pv = fetch(TP_.prb, (size_t)3 * TP_.nprobe * T, K, stream_, d2h_bytes_);
+        const std::string base = d.filename.substr(0, d.filename.size() >= 4 ? d.filename.size() - 4 : 0);
+        const std::string fn = (outdir_.empty() ? "" : outdir_ + "/") + base + "_probes.dat";
+        FILE* pf = std::fopen(fn.c_str(), "w");
+        if (!pf) throw std::runtime_error("cannot write " + fn);
+        std::fprintf(pf, " number of point probes = %12d\n", TP_.nprobe);
+        static const char* cn[3] = {"Ex", "Ey", "Ez"};
+        for (int q = 0; q < TP_.nprobe; q++)
+            for (int c = 0; c < 3; c++) {
+                std::fprintf(pf, " point probe %12d %s at cell%12d%12d%12d\n", q + 1, cn[c], TP_.prb_idx[q][0],
+                             TP_.prb_idx[q][1], TP_.prb_idx[q][2]);
+                for (int n = 0; n < T; n++) wline(pf, pv[((size_t)q * 3 + c) * T + n], K);
+            }
+        std::fclose(pf);
+    }
+
     // video slices, one Fortran unformatted record per file, ref :8788-8807
     if (TP_.video) {
         const char* nm[6] = {"Ex", "Hx", "Ey", "Hy", "Ez", "Hz"};

@@ -77,6 +77,11 @@ struct TapDev {
     int ff_pc;                  // phase-centre sample
     int ic, jc, kc;
     void* pc[6];                // Ex,Ey,Ez,Hx,Hy,Hz per step (+1)
+    // point probes (extension `probe i j k`): the phase-centre sample's
+    // cell-centred Ex, Ey, Ez at each probe cell, every step
+    int nprobe;
+    int prb_idx[AEM_MAX_PROBES][3];
+    void* prb;                  // [probe][component][step]
     int video;                  // 2-D slice export
     int slice_dir, slice_loc, v1, v2;
     void* vid[6];               // Ex,Hx,Ey,Hy,Ez,Hz each (v1, v2, steps)

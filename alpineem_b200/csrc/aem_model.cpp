@@ -386,24 +386,31 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
     // CPML tables, ref :3404-3577, den_*, ref :3586-3666
     const float dl[3] = {d.dx, d.dy, d.dz};
     float kap_e[3][2][AEM_MAX_PML + 1] = {}, kap_h[3][2][AEM_MAX_PML + 1] = {};
+    // g^m as the reference writes it for m = 3, ((g*g)*g); other orders
+    // (extension cpml_grading) multiply on in the same left-to-right order
+    auto gpow = [&](float g) {
+        float p = g;
+        for (int q = 1; q < d.cpml_m; q++) p = p * g;
+        return p;
+    };
     for (int a = 0; a < 3; a++)
         for (int s = 0; s < 2; s++) {
             int n = d.npml[a][s];
             if (n > AEM_MAX_PML) throw DeckError("CPML too thick");
             for (int i = 1; i <= n; i++) {
                 float g = (float)(n - i) / ((float)n - 1.0f);
-                float sg = d.sig_max[a] * (g * g * g);
+                float sg = d.sig_max[a] * gpow(g);
                 float al = d.alpha_max * (((float)i - 1.0f) / ((float)n - 1.0f));
-                float ka = 1.0f + (d.kappa_max - 1.0f) * (g * g * g);
+                float ka = 1.0f + (d.kappa_max - 1.0f) * gpow(g);
                 float b = std::exp(-((sg / ka + al) * dt / kEp0));
                 float c = (sg == 0.0f && al == 0.0f && i == n) ? 0.0f : sg * (b - 1.0f) / (sg + ka * al) / ka;
                 m.be[a][s][i - 1] = b; m.ce[a][s][i - 1] = c; kap_e[a][s][i] = ka;
             }
             for (int i = 1; i <= n - 1; i++) {
                 float g = ((float)(n - i) - 0.5f) / ((float)n - 1.0f);
-                float sg = d.sig_max[a] * (g * g * g);
+                float sg = d.sig_max[a] * gpow(g);
                 float al = d.alpha_max * (((float)i - 0.5f) / ((float)n - 1.0f));
-                float ka = 1.0f + (d.kappa_max - 1.0f) * (g * g * g);
+                float ka = 1.0f + (d.kappa_max - 1.0f) * gpow(g);
                 float b = std::exp(-((sg / ka + al) * dt / kEp0));
                 float c = sg * (b - 1.0f) / (sg + ka * al) / ka;
                 m.bh[a][s][i - 1] = b; m.ch[a][s][i - 1] = c; kap_h[a][s][i] = ka;

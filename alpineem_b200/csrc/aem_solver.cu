@@ -94,9 +94,11 @@ void Solver::init() {
         setup_taps();
         setup_full();
         setup_fused();
-        if (m_.d.ext_watchdog > 0) wd_flag_ = (int*)alloc(sizeof(int));
         AEM_CUDA(cudaStreamSynchronize(stream_));
         nstate_ = bufs_.size();
+        // the watchdog flag is scratch, not run state: allocated after the
+        // state buffers so that checkpoints do not depend on the watchdog
+        if (m_.d.ext_watchdog > 0) wd_flag_ = (int*)alloc(sizeof(int));
     } catch (...) {
         release();  // a throwing constructor runs no destructor
         throw;
@@ -600,6 +602,19 @@ void Solver::setup_taps() {
         T.v2 = d.vid2;
         for (int q = 0; q < 6; q++) T.vid[q] = alloc((size_t)T.v1 * T.v2 * d.steps * es_);
     }
+    if (!d.ext_probes.empty()) {
+        const int n[3] = {d.nx, d.ny, d.nz};
+        T.nprobe = (int)d.ext_probes.size();
+        for (int q = 0; q < T.nprobe; q++)
+            for (int a = 0; a < 3; a++) {
+                const int v = d.ext_probes[q][a];
+                if (v < 1 || v > n[a])
+                    throw DeckError("extension probe " + std::to_string(q + 1) + ": cell index outside 1..n on axis " +
+                                    std::to_string(a));
+                T.prb_idx[q][a] = v;
+            }
+        T.prb = alloc((size_t)3 * T.nprobe * d.steps * es_);
+    }
     dft_series_.clear();
     if (!d.ext_dft_freqs.empty()) {
         // series in the order of the probe kinds: plane sums, then port voltages
@@ -766,8 +781,11 @@ void Solver::read_probe(int kind, int index, int first, int n, double* re, doubl
         if (!TP_.plane_sum) throw std::invalid_argument("the deck has no reflection/transmission planes");
         if (kind >= 3 && !m_.d.kmax) throw std::invalid_argument("TM plane sums (kinds 3, 4) exist in kmax runs only");
         src = kind == 1 ? TP_.refl : kind == 2 ? TP_.trans : kind == 3 ? TP_.refl_tm : TP_.trans_tm;
+    } else if (kind == 6) {
+        if (index < 0 || index >= 3 * TP_.nprobe) throw std::invalid_argument("no such point probe component (index 3 p + c)");
+        src = (const char*)TP_.prb + (size_t)index * m_.d.steps * es_;
     } else {
-        throw std::invalid_argument("probe kind must be 1..5");
+        throw std::invalid_argument("probe kind must be 1..6");
     }
     if (first < 1 || n < 0 || first - 1 + n > done_) throw std::invalid_argument("steps outside those run so far");
     std::vector<char> buf((size_t)n * es_);
@@ -990,6 +1008,14 @@ void Solver::checkpoint_load(const std::string& path) {
             match = n == (long long)buf_bytes_[b];
         }
         if (!match) throw std::invalid_argument("checkpoint '" + path + "' was not written by a run of this deck");
+        // the whole payload must be there before any buffer is overwritten,
+        // so that a truncated file leaves the handle as it was
+        const long pos = std::ftell(f);
+        long long need = 0;
+        for (size_t b = 0; b < nstate_; b++) need += (long long)buf_bytes_[b];
+        if (pos < 0 || std::fseek(f, 0, SEEK_END) != 0 || (long long)std::ftell(f) - pos < need ||
+            std::fseek(f, pos, SEEK_SET) != 0)
+            throw std::invalid_argument("checkpoint '" + path + "' is truncated");
         AEM_CUDA(cudaStreamSynchronize(stream_));
         release_graph();
         AEM_CUDA(cudaMallocHost(&stage, CKPT_CHUNK));

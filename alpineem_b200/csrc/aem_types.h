@@ -27,6 +27,7 @@
 #define AEM_MAX_FF_ANGLES 4096
 #define AEM_MAX_DFT_FREQS 4096
 #define AEM_MAX_DFT_SERIES (4 + AEM_MAX_PORTS)
+#define AEM_MAX_PROBES 64
 
 // Per-material constants (cell properties), ref materials_properties(:,:,:)
 struct AemMaterial {

@@ -326,287 +326,14 @@ __global__ void __launch_bounds__(256) k_yee(const __grid_constant__ AemParams P
 }
 
 // ---------------------------------------------------------------------------
-// k_yee_pipe: the same fused step for grids without x/y periodicity, with
-// every plane's inputs staged through shared memory by asynchronous copies.
-// A CTA owns a 64 x 8 (x, y) column tile and marches a z chunk.  For plane
-// p, one ring slot holds E_old(p) on rows y0-1 .. y0+8 and x0-4 .. x0+67,
-// H_old(p) on rows y0-1 .. y0+7 and x0-4 .. x0+63, and the material ids of
-// rows y0-1 .. y0+7, x0-16 .. x0+63 (16-byte aligned chunks; chunks off the
-// grid are zero-filled, never read).  Plane k+2 is requested while plane k
-// is computed, so two planes of copies are in flight per CTA.  Per plane:
-//   1. H_new(k) on the tile plus its -x column and -y row (65 x 9 cells)
-//      into shared memory; owned cells also go to H2 / psi_h2;
-//   2. E_new(k) of the 64 x 8 owned cells from H_new(k), H_new(k-1) (the
-//      other half of the double-buffered H_new tile) and E_old(k) -> E2.
-// Five slots let the copy of plane k+2 go into the slot of plane k-3, which
-// no thread reads after plane k-2, so two barriers per plane suffice.
-constexpr int YP_TX = 64, YP_TY = 8, YP_ZC = 64, YP_SLOTS = 5;
-constexpr int YP_EW = YP_TX + 8, YP_ER = YP_TY + 2;   // E tile: 72 x 10
-constexpr int YP_HW = YP_TX + 4, YP_HR = YP_TY + 1;   // H tile: 68 x 9
-constexpr int YP_IW = YP_TX + 16;                     // id tile: 80 bytes x 9 rows
-constexpr int YP_SLOT_F = 3 * YP_ER * YP_EW + 3 * YP_HR * YP_HW;  // floats per slot (E, H)
-constexpr int YP_SLOT_B = YP_SLOT_F * 4 + YP_HR * YP_IW;          // bytes per slot
-constexpr int YP_HN_F = 3 * YP_HR * YP_HW;                        // floats of one H_new tile
-constexpr size_t YP_SMEM = (size_t)YP_SLOTS * YP_SLOT_B + 2 * (size_t)YP_HN_F * 4;
-
-__device__ inline void cp16(void* smem, const void* gmem, bool valid) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
-}
-__device__ inline void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ inline void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// request plane p (already wrapped; -1 / SZ = absent) into ring slot `slot`
-__device__ inline void yp_issue(const AemParams& P, unsigned char* smem, int slot, int p, int x0, int y0) {
-    float* E = reinterpret_cast<float*>(smem + (size_t)slot * YP_SLOT_B);
-    float* H = E + 3 * YP_ER * YP_EW;
-    unsigned char* I = smem + (size_t)slot * YP_SLOT_B + YP_SLOT_F * 4;
-    const bool pv = p >= 0 && p < P.SZ;
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    const int nE = 3 * YP_ER * (YP_EW / 4), nH = 3 * YP_HR * (YP_HW / 4), nI = YP_HR * (YP_IW / 16);
-    for (int q = tid; q < nE + nH + nI; q += nt) {
-        if (q < nE) {
-            const int c = q / (YP_ER * (YP_EW / 4)), r = (q / (YP_EW / 4)) % YP_ER, ch = q % (YP_EW / 4);
-            const int x = x0 - 4 + 4 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 4 <= P.PX && y >= 0 && y < P.SY;
-            const float* src = reinterpret_cast<const float*>(P.E[c]) + (ok ? lin(P, x, y, p) : 0);
-            cp16(E + (c * YP_ER + r) * YP_EW + 4 * ch, src, ok);
-        } else if (q < nE + nH) {
-            const int t = q - nE;
-            const int c = t / (YP_HR * (YP_HW / 4)), r = (t / (YP_HW / 4)) % YP_HR, ch = t % (YP_HW / 4);
-            const int x = x0 - 4 + 4 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 4 <= P.PX && y >= 0 && y < P.SY;
-            const float* src = reinterpret_cast<const float*>(P.H[c]) + (ok ? lin(P, x, y, p) : 0);
-            cp16(H + (c * YP_HR + r) * YP_HW + 4 * ch, src, ok);
-        } else {
-            const int t = q - nE - nH;
-            const int r = t / (YP_IW / 16), ch = t % (YP_IW / 16);
-            const int x = x0 - 16 + 16 * ch, y = y0 - 1 + r;
-            const bool ok = pv && x >= 0 && x + 16 <= P.PX && y >= 0 && y < P.SY;
-            const unsigned char* src = P.cell + (ok ? lin(P, x, y, p) : 0);
-            cp16(I + r * YP_IW + 16 * ch, src, ok);
-        }
-    }
-}
-
-// H_new of cell (px,py,pz) from old values already at hand (k_update_h's
-// expressions); psi read from psi_h, written to psi_h2 when `store`
-__device__ inline void h_cell_v(const AemParams& P, int px, int py, int pz, const HNb& e, float hx0, float hy0,
-                                float hz0, bool store, float& hxv, float& hyv, float& hzv) {
-    const int i = px + 1, j = py + 1, k = pz + 1;
-    const float DB = P.DB;
-    const float dhx = P.den_h[0][i - 1], dhy = P.den_h[1][j - 1], dhz = P.den_h[2][k - 1];
-    const int qx_lo = (i <= P.npml[0][0] - 1) ? i : 0, qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
-    const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0, qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
-    const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0, qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
-    hxv = hx0 + DB * ((e.ez - e.ez_jp) * dhy + (e.ey_kp - e.ey) * dhz);
-    hyv = hy0 + DB * ((e.ez_ip - e.ez) * dhx + (e.ex - e.ex_kp) * dhz);
-    hzv = hz0 + DB * ((e.ey - e.ey_ip) * dhx + (e.ex_jp - e.ex) * dhy);
-    if (qx_lo | qx_hi | qy_lo | qy_hi | qz_lo | qz_hi) {
-        if (qy_lo) hxv = hxv + DB * psi_term(P.psi_h[0][1][0], P.psi_h2[0][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], e.ez - e.ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-        if (qy_hi) hxv = hxv + DB * psi_term(P.psi_h[0][1][1], P.psi_h2[0][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], e.ez - e.ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-        if (qz_lo) hxv = hxv + DB * psi_term(P.psi_h[0][2][0], P.psi_h2[0][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], e.ey_kp - e.ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-        if (qz_hi) hxv = hxv + DB * psi_term(P.psi_h[0][2][1], P.psi_h2[0][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], e.ey_kp - e.ey, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-        if (qx_lo) hyv = hyv + DB * psi_term(P.psi_h[1][0][0], P.psi_h2[1][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], e.ez_ip - e.ez, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-        if (qx_hi) hyv = hyv + DB * psi_term(P.psi_h[1][0][1], P.psi_h2[1][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], e.ez_ip - e.ez, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-        if (qz_lo) hyv = hyv + DB * psi_term(P.psi_h[1][2][0], P.psi_h2[1][2][0], store, P.bh[2][0][qz_lo - 1], P.ch[2][0][qz_lo - 1], e.ex - e.ex_kp, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
-        if (qz_hi) hyv = hyv + DB * psi_term(P.psi_h[1][2][1], P.psi_h2[1][2][1], store, P.bh[2][1][qz_hi - 1], P.ch[2][1][qz_hi - 1], e.ex - e.ex_kp, P.del[2], psi_idx(P, 2, qz_hi, px, py, pz, P.npml[2][1]));
-        if (qx_lo) hzv = hzv + DB * psi_term(P.psi_h[2][0][0], P.psi_h2[2][0][0], store, P.bh[0][0][qx_lo - 1], P.ch[0][0][qx_lo - 1], e.ey - e.ey_ip, P.del[0], psi_idx(P, 0, qx_lo, px, py, pz, P.npml[0][0]));
-        if (qx_hi) hzv = hzv + DB * psi_term(P.psi_h[2][0][1], P.psi_h2[2][0][1], store, P.bh[0][1][qx_hi - 1], P.ch[0][1][qx_hi - 1], e.ey - e.ey_ip, P.del[0], psi_idx(P, 0, qx_hi, px, py, pz, P.npml[0][1]));
-        if (qy_lo) hzv = hzv + DB * psi_term(P.psi_h[2][1][0], P.psi_h2[2][1][0], store, P.bh[1][0][qy_lo - 1], P.ch[1][0][qy_lo - 1], e.ex_jp - e.ex, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
-        if (qy_hi) hzv = hzv + DB * psi_term(P.psi_h[2][1][1], P.psi_h2[2][1][1], store, P.bh[1][1][qy_hi - 1], P.ch[1][1][qy_hi - 1], e.ex_jp - e.ex, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
-    }
-}
-
-// H_new(plane pz) on the 65 x 9 region (own tile + -x column + -y row) into
-// shared `hn` ([3][9][68], x offset 3); owned, updated cells also to H2
-__device__ inline void yp_h_region(const AemParams& P, const float* E0, const float* E1, const float* Ho, float* hn,
-                                   int pz, int x0, int y0, int hxm, int hym, int hzm, bool store) {
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    for (int q = tid; q < (YP_TX + 1) * (YP_TY + 1); q += nt) {
-        const int r = q / (YP_TX + 1), col = q % (YP_TX + 1);
-        const int x = x0 - 1 + col, y = y0 - 1 + r;
-        const int ei = r * YP_EW + col + 3, hi = r * YP_HW + col + 3;
-        const float hx0 = Ho[hi], hy0 = Ho[YP_HR * YP_HW + hi], hz0 = Ho[2 * YP_HR * YP_HW + hi];
-        float hx = hx0, hy = hy0, hz = hz0;
-        if (x >= 0 && x <= hxm && y >= 0 && y <= hym && pz <= hzm) {
-            HNb e;
-            const float* Ex = E0;
-            const float* Ey = E0 + YP_ER * YP_EW;
-            const float* Ez = E0 + 2 * YP_ER * YP_EW;
-            e.ex = Ex[ei]; e.ey = Ey[ei]; e.ez = Ez[ei];
-            e.ex_jp = Ex[ei + YP_EW]; e.ez_jp = Ez[ei + YP_EW];
-            e.ey_ip = Ey[ei + 1]; e.ez_ip = Ez[ei + 1];
-            e.ex_kp = E1[ei]; e.ey_kp = E1[YP_ER * YP_EW + ei];
-            const bool own = store && col >= 1 && r >= 1;
-            h_cell_v(P, x, y, pz, e, hx0, hy0, hz0, own, hx, hy, hz);
-            if (own) {
-                const long long c = lin(P, x, y, pz);
-                stf(P.H2[0], c, hx);
-                stf(P.H2[1], c, hy);
-                stf(P.H2[2], c, hz);
-            }
-        }
-        hn[hi] = hx;
-        hn[YP_HR * YP_HW + hi] = hy;
-        hn[2 * YP_HR * YP_HW + hi] = hz;
-    }
-}
-
-__global__ void __launch_bounds__(256, 2) k_yee_pipe(const __grid_constant__ AemParams P) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    float* hn_base = reinterpret_cast<float*>(smem + (size_t)YP_SLOTS * YP_SLOT_B);
-    const int lane = threadIdx.x, ty = threadIdx.y;
-    const int x0 = blockIdx.x * YP_TX, y0 = blockIdx.y * YP_TY;
-    const int z0 = blockIdx.z * YP_ZC, z1 = min(P.SZ, z0 + YP_ZC);
-    const int hxm = P.SX - 2, hym = P.SY - 2, hzm = P.per[2] ? P.SZ - 1 : P.SZ - 2;
-    auto zw = [&](int p) {  // wrapped plane index, -1 / SZ when absent
-        if (P.per[2]) return (p % P.SZ + P.SZ) % P.SZ;
-        return p;
-    };
-    auto slot_of = [&](int p) { return ((p % YP_SLOTS) + YP_SLOTS) % YP_SLOTS; };
-    auto Eslot = [&](int p) { return reinterpret_cast<const float*>(smem + (size_t)slot_of(p) * YP_SLOT_B); };
-    auto Hslot = [&](int p) { return Eslot(p) + 3 * YP_ER * YP_EW; };
-    auto Islot = [&](int p) { return smem + (size_t)slot_of(p) * YP_SLOT_B + YP_SLOT_F * 4; };
-    auto Hn = [&](int p) { return hn_base + (size_t)(((p % 2) + 2) % 2) * YP_HN_F; };
-
-    // prologue: planes z0-1, z0, z0+1; H_new(z0-1) when a plane lies below
-    const bool below = P.per[2] || z0 > 0;
-    yp_issue(P, smem, slot_of(z0 - 1), below ? zw(z0 - 1) : -1, x0, y0);
-    cp_commit();
-    yp_issue(P, smem, slot_of(z0), zw(z0), x0, y0);
-    cp_commit();
-    yp_issue(P, smem, slot_of(z0 + 1), zw(z0 + 1), x0, y0);
-    cp_commit();
-    cp_wait<0>();
-    __syncthreads();
-    // (the plane below belongs to the chunk underneath: recomputed, not stored)
-    if (below) yp_h_region(P, Eslot(z0 - 1), Eslot(z0), Hslot(z0 - 1), Hn(z0 - 1), zw(z0 - 1), x0, y0, hxm, hym, hzm, false);
-
-    // owned cells of this thread: row ty, x = x0 + lane and x0 + 32 + lane
-    const int py = y0 + ty, j = py + 1;
-    const bool row_ok = py < P.SY;
-    const float dey = row_ok ? P.den_e[1][j - 1] : 0.0f;
-    const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
-
-    for (int k = z0; k < z1; k++) {
-        const int pz = zw(k);
-        // request plane k+2 (its slot last served plane k-3), then wait for k+1
-        yp_issue(P, smem, slot_of(k + 2), k + 2 <= z1 ? zw(k + 2) : -1, x0, y0);
-        cp_commit();
-        cp_wait<1>();
-        __syncthreads();
-        yp_h_region(P, Eslot(k), Eslot(k + 1), Hslot(k), Hn(k), pz, x0, y0, hxm, hym, hzm, true);
-        __syncthreads();
-
-        const float* E0 = Eslot(k);
-        const float* hn = Hn(k);
-        const float* hp = Hn(k - 1);
-        const unsigned char* I0 = Islot(k);
-        const unsigned char* I1 = Islot(k - 1);
-        const int kk = pz + 1;
-        const float dez = P.den_e[2][kk - 1];
-        const int qzl = (kk >= 2 && kk <= P.npml[2][0]) ? kk : 0, qzh = (kk >= P.Z + 1 - P.npml[2][1] && kk <= P.Z - 1) ? P.Z + 1 - kk : 0;
-        for (int h = 0; h < 2; h++) {
-            const int cx = lane + 32 * h, px = x0 + cx, i = px + 1;
-            if (!row_ok || px >= P.SX) continue;
-            const bool ex_u = px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
-            const bool ey_u = px >= 1 && px <= P.SX - 2 && py <= P.SY - 2 && (P.per[2] || (pz >= 1 && pz <= P.SZ - 2));
-            const bool ez_u = px >= 1 && px <= P.SX - 2 && py >= 1 && py <= P.SY - 2 && (P.per[2] || pz <= P.SZ - 2);
-            if (!(ex_u || ey_u || ez_u)) continue;
-            const int r = ty + 1, col = cx + 1;
-            const int hi = r * YP_HW + col + 3, ei = r * YP_EW + col + 3, ii = r * YP_IW + cx + 16;
-            const float hx = hn[hi], hy = hn[YP_HR * YP_HW + hi], hz = hn[2 * YP_HR * YP_HW + hi];
-            const float hz_im = hn[2 * YP_HR * YP_HW + hi - 1], hy_im = hn[YP_HR * YP_HW + hi - 1];
-            const float hz_jm = hn[2 * YP_HR * YP_HW + hi - YP_HW], hx_jm = hn[hi - YP_HW];
-            const float hxp = hp[hi], hyp = hp[YP_HR * YP_HW + hi];
-            const float dex = P.den_e[0][i - 1];
-            const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
-            const bool unavg = i == 1 || j == 1 || (!P.per[2] && kk == 1);
-            const int idc = unavg ? 0 : I0[ii], idx_ = unavg ? 0 : I0[ii - 1], idy_ = unavg ? 0 : I0[ii - YP_IW],
-                      idxy = unavg ? 0 : I0[ii - YP_IW - 1];
-            const int pdc = unavg ? 0 : I1[ii], pdx = unavg ? 0 : I1[ii - 1], pdy = unavg ? 0 : I1[ii - YP_IW];
-            const long long c = lin(P, px, py, pz);
-            if (ex_u) {
-                const float d1 = hz - hz_jm, d2 = hyp - hy;
-                const float curl = d1 * dey + d2 * dez;
-                float ga, gb;
-                edge_gagb(P, 0, idc, idy_, pdc, pdy, ga, gb);
-                float e = ga * E0[ei] + gb * curl;
-                if (qyl) e = e + gb * psi_term(P.psi_e[0][1][0], P.psi_e[0][1][0], true, P.be[1][0][qyl - 1], P.ce[1][0][qyl - 1], d1, P.del[1], psi_idx(P, 1, qyl, px, py, pz, P.npml[1][0]));
-                if (qyh) e = e + gb * psi_term(P.psi_e[0][1][1], P.psi_e[0][1][1], true, P.be[1][1][qyh - 1], P.ce[1][1][qyh - 1], d1, P.del[1], psi_idx(P, 1, qyh, px, py, pz, P.npml[1][1]));
-                if (qzl) e = e + gb * psi_term(P.psi_e[0][2][0], P.psi_e[0][2][0], true, P.be[2][0][qzl - 1], P.ce[2][0][qzl - 1], d2, P.del[2], psi_idx(P, 2, qzl, px, py, pz, P.npml[2][0]));
-                if (qzh) e = e + gb * psi_term(P.psi_e[0][2][1], P.psi_e[0][2][1], true, P.be[2][1][qzh - 1], P.ce[2][1][qzh - 1], d2, P.del[2], psi_idx(P, 2, qzh, px, py, pz, P.npml[2][1]));
-                stf(P.E2[0], c, e);
-            }
-            if (ey_u) {
-                const float d1 = hz_im - hz, d2 = hx - hxp;
-                const float curl = d1 * dex + d2 * dez;
-                float ga, gb;
-                edge_gagb(P, 1, idc, idx_, pdc, pdx, ga, gb);
-                float e = ga * E0[YP_ER * YP_EW + ei] + gb * curl;
-                if (qxl) e = e + gb * psi_term(P.psi_e[1][0][0], P.psi_e[1][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], d1, P.del[0], psi_idx(P, 0, qxl, px, py, pz, P.npml[0][0]));
-                if (qxh) e = e + gb * psi_term(P.psi_e[1][0][1], P.psi_e[1][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], d1, P.del[0], psi_idx(P, 0, qxh, px, py, pz, P.npml[0][1]));
-                if (qzl) e = e + gb * psi_term(P.psi_e[1][2][0], P.psi_e[1][2][0], true, P.be[2][0][qzl - 1], P.ce[2][0][qzl - 1], d2, P.del[2], psi_idx(P, 2, qzl, px, py, pz, P.npml[2][0]));
-                if (qzh) e = e + gb * psi_term(P.psi_e[1][2][1], P.psi_e[1][2][1], true, P.be[2][1][qzh - 1], P.ce[2][1][qzh - 1], d2, P.del[2], psi_idx(P, 2, qzh, px, py, pz, P.npml[2][1]));
-                stf(P.E2[1], c, e);
-            }
-            if (ez_u) {
-                const float d1 = hy - hy_im, d2 = hx_jm - hx;
-                const float curl = d1 * dex + d2 * dey;
-                float ga, gb;
-                edge_gagb(P, 2, idc, idx_, idy_, idxy, ga, gb);
-                float e = ga * E0[2 * YP_ER * YP_EW + ei] + gb * curl;
-                if (qxl) e = e + gb * psi_term(P.psi_e[2][0][0], P.psi_e[2][0][0], true, P.be[0][0][qxl - 1], P.ce[0][0][qxl - 1], d1, P.del[0], psi_idx(P, 0, qxl, px, py, pz, P.npml[0][0]));
-                if (qxh) e = e + gb * psi_term(P.psi_e[2][0][1], P.psi_e[2][0][1], true, P.be[0][1][qxh - 1], P.ce[0][1][qxh - 1], d1, P.del[0], psi_idx(P, 0, qxh, px, py, pz, P.npml[0][1]));
-                if (qyl) e = e + gb * psi_term(P.psi_e[2][1][0], P.psi_e[2][1][0], true, P.be[1][0][qyl - 1], P.ce[1][0][qyl - 1], d2, P.del[1], psi_idx(P, 1, qyl, px, py, pz, P.npml[1][0]));
-                if (qyh) e = e + gb * psi_term(P.psi_e[2][1][1], P.psi_e[2][1][1], true, P.be[1][1][qyh - 1], P.ce[1][1][qyh - 1], d2, P.del[1], psi_idx(P, 1, qyh, px, py, pz, P.npml[1][1]));
-                stf(P.E2[2], c, e);
-            }
-        }
-    }
-    cp_wait<0>();  // no copy may still target this CTA's shared memory at exit
-}
-
 bool yee_fused_ok(const AemParams& P, int gridded_ports) {
     return !P.kmax && !P.tfsf_on && !P.mirror_on && P.nsheet == 0 && P.npoles == 0 && !P.has_drude &&
            !P.kmax_mode_TE && !P.kmax_mode_TM && gridded_ports == 0;
 }
 
-// AEM_YEE_PLAIN=1 keeps the register-only kernel on every grid (A/B timing)
-static bool yee_pipe_disabled() {
-    static const bool off = [] {
-        const char* v = std::getenv("AEM_YEE_PLAIN");
-        return v && *v && std::strcmp(v, "0") != 0;
-    }();
-    return off;
-}
-
-static bool env_flag(const char* name) {
-    const char* v = std::getenv(name);
-    return v && *v && std::strcmp(v, "0") != 0;
-}
-
 int launch_yee(const AemParams& P, cudaStream_t s) {
-    // grids without x/y periodicity: the 4-cells-per-thread kernel
-    // (AEM_YEE_PIPE=1 selects the scalar staged kernel instead)
-    static const bool pipe = env_flag("AEM_YEE_PIPE");
-    if (!P.per[0] && !P.per[1] && !yee_pipe_disabled() && !pipe) return launch_yee4(P, s);
-    if (!P.per[0] && !P.per[1] && !yee_pipe_disabled()) {
-        // the shared-memory limit is a per-device property of the function
-        static bool attr_set[64] = {};
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-            cudaFuncSetAttribute(k_yee_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)YP_SMEM);
-            attr_set[dev] = true;
-        }
-        dim3 blk(32, YP_TY), grd((P.SX + YP_TX - 1) / YP_TX, (P.SY + YP_TY - 1) / YP_TY, (P.SZ + YP_ZC - 1) / YP_ZC);
-        k_yee_pipe<<<grd, blk, YP_SMEM, s>>>(P);
-        return 1;
-    }
+    // grids without x/y periodicity: the TMA-fed 4-cells-per-thread kernel
+    if (!P.per[0] && !P.per[1]) return launch_yee4(P, s);
     dim3 blk(32, YEE_TY), grd((P.SX + 31) / 32, (P.SY + YEE_TY - 1) / YEE_TY, (P.SZ + YEE_ZC - 1) / YEE_ZC);
     k_yee<<<grd, blk, 0, s>>>(P);
     return 1;

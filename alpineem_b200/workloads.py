@@ -62,8 +62,100 @@ def dipole_ellipsoids(n=1024, steps=4000, n_ell=64, seed=2, pml_cells=16, dl="2E
              bulk="optional_geom_bulk.bin",
              objects=[("block", 1, (c, c, c - arm), (1, 1, arm)), ("block", 1, (c, c, c + 1), (1, 1, arm))],
              ports=[("basic", "z", 50, (c, c, c), (1, 1, 1))])
-    ext = "pml_cells %d\ngeometry_bin no\n" % pml_cells
+    # port S11 spectra on the fly at 512 frequencies over the Gaussian
+    # pulse's band (post-processor bounds 0 .. 2.146 f)
+    ext = "pml_cells %d\ngeometry_bin no\ndft_freqs 1e8 %.6g 512\n" % (pml_cells, 2.146 * float(f))
     return d, ext, bulk
+
+
+# CPML profile of the scattering and layered-slab configurations: cubic
+# grading, sigma_max = 0.8 (m+1) / (eta0 d), kappa_max = 1, alpha from 0.05
+# at the inner edge to 0 at the outer wall (the reference's direction)
+BASELINE_CPML = "cpml_grading 3 0.8 1 0.05\n"
+
+
+def pec_sphere(n=96, steps=2000, radius=20, inset=15, seed=0, n_probes=3, dl="5E-3", f="1E9",
+               theta_step=5, factor=0.98 / 0.99):
+    """PEC-sphere scattering: an n^3 grid of `dl` cells with 10 cells of
+    CPML on every face (BASELINE_CPML profile), the TF/SF box `inset` cells
+    in from every edge, an x-polarised differentiated-Gaussian plane wave
+    travelling +z (theta = 0, pol = 270 deg), a PEC sphere (sigma = 1e8, the
+    reference's encoding of a metal volume) of `radius` cells at the grid
+    centre, time-domain far fields at theta = 0..180 in `theta_step` degree
+    steps at phi = 0, and `n_probes` point probes drawn with numpy
+    default_rng(seed) in the scattered-field region (between the CPML and
+    the TF/SF box).  factor = 0.98/0.99 turns the reference's Courant number
+    0.98/sqrt(3) into 0.99/sqrt(3).  With f = 1 GHz the post-processor's
+    band of a differentiated Gaussian (0.183 f .. 3.087 f) is
+    0.18 .. 3.09 GHz.
+
+    Returns (deck, ext_text, probes) with probes a list of (i, j, k)."""
+    rng = np.random.default_rng(seed)
+    npml = 11  # 10 cells of CPML: the reference's npml = cells + 1
+    N = n + 1
+    lo, hi = inset, N - inset
+    probes = []
+    while len(probes) < n_probes:
+        p = tuple(int(v) for v in rng.integers(npml + 1, N - npml - 1, size=3))
+        if all(lo <= v <= hi for v in p):
+            continue  # inside the total-field box
+        probes.append(p)
+    c = n // 2
+    ff = [(t, 0) for t in range(0, 181, theta_step)]
+    d = dict(n=(n, n, n), dl=(dl, dl, dl), steps=steps, factor=repr(factor), f=f, pulse=2, bc=(0, 0, 0, 0, 0, 0),
+             excitation=("plane wave", 1, 0, 0, 0, 270), ff=ff, ffc=(c, c, c), name="data.dat",
+             mats=[("simple", 1, (1, 1, 1), ("1E8", "1E8", "1E8"))],
+             objects=[("sphere", 1, (c, c, c), radius)])
+    ext = BASELINE_CPML + "tfsf_inset %d\n" % inset + "".join("probe %d %d %d\n" % p for p in probes)
+    return d, ext, probes
+
+
+def layered_slab(nxy=128, nz=512, steps=8000, seed=1, n_layers=8, pml_cells=12, dl="1E-3", f="10E9", n_freqs=256,
+                 z0=60):
+    """Dispersive, anisotropic layered slab with a thin sheet: an nxy x nxy
+    x nz unit cell of `dl` cells, periodic in x and y, `pml_cells` of CPML
+    on both z faces (BASELINE_CPML profile), a normally incident
+    x-polarised differentiated-Gaussian plane wave travelling +z.  From
+    z = z0 up: `n_layers` dielectric layers (thickness ~ U{8..40} cells,
+    diagonal eps_r with every axis ~ U[1, 10], sigma ~ U[0, 0.05] S/m,
+    numpy default_rng(seed)), then one 2-pole Drude layer (omega_p ~
+    U[1e10, 5e10] rad/s, gamma ~ U[1e8, 1e10] 1/s, same generator), and a
+    Smith-Maloney sheet of 100 S (0.01 ohm/sq) on the top face of the
+    first layer.  The reflected and transmitted plane sums are recorded
+    every step and their spectra accumulated on the fly at `n_freqs`
+    frequencies from 1 to 30 GHz.  With f = 10 GHz the post-processor's
+    band of the pulse is 1.83 .. 30.9 GHz.
+
+    Returns (deck, ext_text, layers) with layers a list of
+    (z_start, thickness, material id)."""
+    rng = np.random.default_rng(seed)
+    mats, objects, layers = [], [], []
+    z = z0
+    for q in range(n_layers):
+        t = int(rng.integers(8, 41))
+        eps = tuple(float(v) for v in rng.uniform(1.0, 10.0, size=3))
+        sig = float(rng.uniform(0.0, 0.05))
+        mid = 2 + q
+        mats.append(("simple", mid, tuple("%.6f" % v for v in eps), ("%.6f" % sig,) * 3))
+        objects.append(("block", mid, (1, 1, z), (nxy, nxy, t)))
+        layers.append((z, t, mid))
+        z += t
+    t = int(rng.integers(8, 41))
+    poles = [("%.6E" % rng.uniform(1e10, 5e10), "%.6E" % rng.uniform(1e8, 1e10)) for _ in range(2)]
+    mid = 2 + n_layers
+    mats.append(("plasma", mid, (1, 1, 1), (0, 0, 0), poles))
+    objects.append(("block", mid, (1, 1, z), (nxy, nxy, t)))
+    layers.append((z, t, mid))
+    z += t
+    if z >= nz - pml_cells - 6:
+        raise ValueError("the layer stack reaches the CPML; enlarge nz")
+    sheet_z = layers[0][0] + layers[0][1]
+    mats.append(("sheet", 1, "0.01"))
+    d = dict(n=(nxy, nxy, nz), dl=(dl, dl, dl), steps=steps, factor=1, f=f, pulse=2, bc=(1, 1, 1, 1, 0, 0),
+             excitation=("plane wave", 1, 0, 0, 0, 270), name="data.dat", mats=mats, objects=objects,
+             sheets=[("z", 1, sheet_z, (1, 1), (nxy, nxy))])
+    ext = BASELINE_CPML + "pml_cells %d\ndft_freqs 1e9 3e10 %d\n" % (pml_cells, n_freqs)
+    return d, ext, layers
 
 
 # sidecar extension of every kmax_batch instance: on-the-fly spectra of the

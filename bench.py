@@ -50,8 +50,11 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=32)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=1024, help="grid cells per axis of the GPU workload")
-    ap.add_argument("--cpu-n", type=int, default=256, help="grid cells per axis of the CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=8, help="timed steps of the cpu_baseline sample")
+    ap.add_argument("--cpu-n", type=int, default=0,
+                    help="grid cells per axis of the reference arm (0: the GPU grid if host memory allows)")
+    ap.add_argument("--cpu-baseline-n", type=int, default=512, help="grid cells per axis of the cpu_baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the cpu_baseline sample")
+    ap.add_argument("--no-configs", action="store_true", help="skip the scattering and layered-slab measurements")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched kmax-instance measurement")
@@ -61,7 +64,7 @@ def parse_args():
     ap.add_argument("--adjoint-n", type=int, default=192, help="grid cells per axis of the design-gradient workload")
     ap.add_argument("--adjoint-steps", type=int, default=3000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=200, help="steps between forward checkpoints")
-    ap.add_argument("--adjoint-fd", type=int, default=2,
+    ap.add_argument("--adjoint-fd", type=int, default=20,
                     help="design cells checked against FP64 central differences (2 FP64 runs each)")
     return ap.parse_args()
 
@@ -81,20 +84,48 @@ def hbm_peak():
 
 def dram_traffic_ratio():
     """Measured DRAM bytes of one fused Yee launch over its algorithmic bytes,
-    from the committed ncu summary (profiles/yee_update_dipole_ellipsoids.md,
-    line 'dram_traffic_over_algorithmic: X'), or None.  The capture runs a
+    from the committed ncu record profiles/yee_update_dipole_ellipsoids.json
+    (field dram_traffic_over_algorithmic), or None.  The capture runs a
     smaller instance of the workload; the ratio (halo re-reads of the tiles)
     carries over to the full grid, the per-cell bytes do not (the CPML share
     of the cells shrinks as the grid grows)."""
-    p = os.path.join(ROOT, "profiles", "yee_update_dipole_ellipsoids.md")
+    p = os.path.join(ROOT, "profiles", "yee_update_dipole_ellipsoids.json")
     try:
         with open(p) as f:
+            return float(json.load(f)["dram_traffic_over_algorithmic"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def host_mem_available():
+    """Bytes of host memory available (MemAvailable), or None."""
+    try:
+        with open("/proc/meminfo") as f:
             for line in f:
-                if line.startswith("dram_traffic_over_algorithmic:"):
-                    return float(line.split(":", 1)[1])
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
     except OSError:
         pass
     return None
+
+
+def reference_grid(n):
+    """Grid of the CPU runs: the GPU workload's own n^3 when the oracle's
+    working set (about 52 B per cell plus the bulk file) fits in the host's
+    available memory with a margin, else the largest power-of-two fraction
+    of n that does."""
+    avail = host_mem_available() or 0
+    m = n
+    while m > 128 and 64 * m ** 3 > 0.8 * avail:
+        m //= 2
+    return m
+
+
+def workload_config(n):
+    """The `config` object of both arms' JSON lines for an n^3 grid."""
+    return {"workload": WORKLOAD, "grid": [n, n, n], "cells": n ** 3, "cpml_cells": 16, "ellipsoids": 64,
+            "far_field_angles": 684, "s11_frequencies": 512, "deck_steps": 4000,
+            "l2": "no flush: the fields and tables (about 28 GB at 1024^3) are far above the 126 MB L2"}
 
 
 class ClockSampler:
@@ -181,20 +212,25 @@ def oracle_sample(n, warm, steps, threads=None):
 
 
 def reference_arm(args):
-    """The reference's CPU path on this box's host cores: the oracle on a
-    cpu-n^3 sample of the workload, warm-up then --steps timed steps."""
+    """The reference's CPU path on this box's host cores: the oracle on the
+    GPU arm's own grid when host memory allows (else a power-of-two fraction
+    of it, reference_grid), 1 untimed warm-up step, then min(--steps, 3)
+    timed steps at 1024^3 (a step there is seconds of work on all host
+    threads) or --steps after --warmup on smaller grids."""
     rank, _, world = ranks()
     if rank != 0:
         return
-    v, threads, cells = oracle_sample(args.cpu_n, args.warmup, args.steps)
-    n = args.cpu_n
-    sample = ("%d^3 instance of the workload (%d cells, 64 ellipsoids, 684 far-field angles, 16-cell CPML), "
-              "%d timed steps after %d warm-up" % (n, cells, args.steps, args.warmup))
+    n = args.cpu_n or reference_grid(args.n)
+    warm, steps = (1, min(args.steps, 3)) if n >= 1024 else (args.warmup, args.steps)
+    v, threads, cells = oracle_sample(n, warm, steps)
+    sample = ("%d^3 instance of the workload (%d cells, 64 ellipsoids, 684 far-field angles, 16-cell CPML, "
+              "port spectra at 512 frequencies), %d timed steps after %d warm-up; grid %s"
+              % (n, cells, steps, warm, "= the GPU arm's" if n == args.n else
+                 "reduced from %d^3: host memory" % args.n))
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(cells / (v * 1e6) * 1e3, 3),
+            "steps": steps, "warmup": warm, "ms_per_step": round(cells / (v * 1e6) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [n, n, n], "cpml_cells": 16, "ellipsoids": 64,
-                       "far_field_angles": 684, "deck_steps": 4000},
+            "config": workload_config(n),
             "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -339,6 +375,43 @@ def adjoint_gradient(args, max_over_ranks):
     return out
 
 
+def config_runs(max_over_ranks, world):
+    """The scattering (workloads.pec_sphere: 96^3, 2000 steps) and layered
+    unit-cell (workloads.layered_slab: 128 x 128 x 512, 8000 steps)
+    configurations, each run whole on the device: Mcell-updates/s of all
+    its steps (CUDA events on the solver's stream, every rank a replica),
+    the per-phase split, and the update kernels' HBM roofline (the
+    algorithmic bytes of the Yee/CPML update over their summed event time)."""
+    import alpineem_b200 as ab
+    from alpineem_b200 import workloads
+    from alpineem_b200.deck import deck_text
+    peak, _ = hbm_peak()
+    out = {}
+    for name, (deck, ext, _) in (("pec_sphere", workloads.pec_sphere()), ("layered_slab", workloads.layered_slab())):
+        tmp = tempfile.mkdtemp(prefix="aem_cfg_")
+        sim = ab.Simulation(deck_text=deck_text(deck), ext_text=ext, outdir=tmp)
+        cells, bytes_step = sim.workload
+        steps = sim.steps[1]
+        sim.synchronize()
+        sim.profile(True)
+        t0 = time.perf_counter()
+        sim.run(steps)
+        sim.synchronize()
+        wall = max_over_ranks(time.perf_counter() - t0)
+        prof = sim.profile_read()
+        sim.profile(False)
+        sim.close()
+        dev_ms = max_over_ranks(sum(v[0] for v in prof.values()))
+        t_upd = (prof["update_h"][0] + prof["update_e"][0] + prof["yee"][0]) / steps / 1e3
+        out[name] = {"grid": list(deck["n"]), "steps": steps, "cells": cells,
+                     "device_mcell_updates_per_s": round(world * cells * steps / (dev_ms / 1e3) / 1e6, 1),
+                     "wall_mcell_updates_per_s": round(world * cells * steps / wall / 1e6, 1),
+                     "phases_ms_per_step": {k: round(v[0] / steps, 5) for k, v in prof.items() if v[1]},
+                     "update_roofline_frac": round(bytes_step / t_upd / 1e9 / peak, 4),
+                     "update_path": "fused k_yee4" if prof["yee"][1] else "k_update_h + k_update_e"}
+    return out
+
+
 def ours(args):
     import torch
     import alpineem_b200 as ab
@@ -376,8 +449,11 @@ def ours(args):
     t_setup = time.time() - t0
     cells, bytes_step = sim.workload
 
-    # warm-up, then K timed steps; per-phase events bracket every launch
+    # warm-up (its far-field contributions binned before the timed region),
+    # then K timed steps whose own contributions are binned inside it;
+    # per-phase events bracket every launch
     sim.run(W)
+    sim.flush()
     sim.synchronize()
     sim.profile(True)
     stream = torch.cuda.ExternalStream(sim.stream)
@@ -394,6 +470,11 @@ def ours(args):
     ms = ev0.elapsed_time(ev1)
     launches = sim.launches - launches0
     prof = sim.profile_read()
+    ff_cells, ff_angles = sim.far_field_size
+    # steady state of the far-field binning: one whole 32-step batch
+    sim.profile(True)
+    sim.run(32)
+    steady = sim.profile_read()
     sim.profile(False)
     ms_max = max_over_ranks(ms)
     value = world * cells * K / (ms_max / 1e3) / 1e6
@@ -403,19 +484,24 @@ def ours(args):
     peak, peak_kind = hbm_peak()
     achieved = bytes_step / t_yee / 1e9
     ratio = dram_traffic_ratio()
-    kname = "k_yee (fused H+E step)" if prof["yee"][1] else "k_update_h + k_update_e (one Yee step)"
+    kname = "k_yee4 (fused H+E step, TMA-fed)" if prof["yee"][1] else "k_update_h + k_update_e (one Yee step)"
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": round(ratio * bytes_step) if ratio else None,
+                "traffic_source": "profiles/yee_update_dipole_ellipsoids.json (ncu DRAM bytes / algorithmic bytes "
+                                  "of a 384^3 capture, times this launch's algorithmic bytes)",
                 "algorithmic_bytes": round(bytes_step), "bytes_per_cell_update": round(bytes_step / cells, 2)}
     phases = {k: round(v[0] / K, 4) for k, v in prof.items() if v[1]}
-    ff_cells, ff_angles = sim.far_field_size
     far_field = None
     if prof["ff_bin"][1] and prof["ff_bin"][0] > 0:
         contrib = ff_cells * ff_angles
         far_field = {"metric": "binned far-field contributions/s", "face_cells": ff_cells, "angles": ff_angles,
-                     "contributions_per_step": contrib, "ms_per_step": round(prof["ff_bin"][0] / K, 4),
-                     "value": round(world * contrib / (prof["ff_bin"][0] / K / 1e3), 1)}
+                     "contributions_per_step": contrib, "batch_steps": 32,
+                     "timed_ms_per_step": round(prof["ff_bin"][0] / K, 4),
+                     "timed_note": "the K timed steps are binned in ceil(K/32) batches inside the timed region",
+                     "steady_ms_per_step": round(steady["ff_bin"][0] / 32, 4),
+                     "value": round(world * contrib / (steady["ff_bin"][0] / 32 / 1e3), 1)}
+    n_s11 = len(sim.spectrum("port_voltage", 0, n=4096)[0])  # on-the-fly S11 spectra, accumulated every step
     sim.close()
     del sim
 
@@ -450,25 +536,27 @@ def ours(args):
     if not args.no_adjoint:
         adjoint = adjoint_gradient(args, max_over_ranks)
 
+    configs = None
+    if not args.no_configs:
+        configs = config_runs(max_over_ranks, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, threads, ccells = oracle_sample(args.cpu_n, 1, args.cpu_steps)
+        cn = min(args.cpu_baseline_n, reference_grid(args.n))
+        v, threads, ccells = oracle_sample(cn, 1, args.cpu_steps)
         cpu = {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": "oracle (C/OpenMP restatement of the reference loop) on a %d^3 instance of the workload "
                          "(%d cells, same CPML, ellipsoids, port and 684 far-field angles), %d timed steps after 1 warm-up"
-                         % (args.cpu_n, ccells, args.cpu_steps)}
+                         % (cn, ccells, args.cpu_steps)}
 
     if rank == 0:
+        config = dict(workload_config(args.n), parallelism="replicas" if world > 1 else "single")
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": round(ms_max / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "grid": [args.n] * 3, "cells": cells, "cpml_cells": 16,
-                           "ellipsoids": 64, "far_field_angles": 684, "deck_steps": deck["steps"],
-                           "l2": "no flush: 28 GB of resident fields and tables, far above the 126 MB L2",
-                           "parallelism": "replicas" if world > 1 else "single"},
+                "dtype": "f32", "data": "synthetic", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": launches, "phases_ms_per_step": phases, "far_field": far_field,
-                "batched_kmax": batched, "adjoint": adjoint,
+                "s11_frequencies": n_s11, "configs": configs, "batched_kmax": batched, "adjoint": adjoint,
                 "setup_s": round(t_setup, 2), "workload_gen_s": round(t_gen, 2)}
         print(json.dumps(line), flush=True)
     if dist:

@@ -57,6 +57,16 @@ int aem_create_from_file(const char* inputs_path, int mode, const char* outdir, 
  * per line, as in the optional "<inputs>.b200" sidecar:
  *   pml_cells N      CPML thickness in cells (reference: 10, :1305-1318)
  *   geometry_bin no  skip building and writing <name>_geometry.bin
+ *   cpml_grading m sigma_factor kappa_max alpha_max
+ *                    CPML profile of order m with sigma_max =
+ *                    sigma_factor (m+1) / (eta0 d) (reference: its fixed
+ *                    profile, :1685-1706, :3404-3577)
+ *   tfsf_inset N     TF/SF planes at index N and X-N (reference: npml+3,
+ *                    :1386-1397)
+ *   probe i j k      cell-centred Ex, Ey, Ez at cell (i, j, k) every step,
+ *                    written to <name>_probes.dat (repeatable, at most 64)
+ *   dft_freqs f0 f1 n   on-the-fly spectra (see aem_read_spectrum)
+ *   watchdog K       check the fields for non-finite values every K steps
  * `bulk` replaces the bulk geometry file the deck names (:2051-2055):
  * bulk_count float32 material ids, x fastest, (nx, ny, nz) cells; NULL/0
  * when the deck has none.  Side files (gridded feeds) and outputs resolve
@@ -94,8 +104,11 @@ int aem_run_batch(aem_handle* const* handles, int count, int nsteps, int steps_p
  * that aem_write_outputs applies: kind 5 = voltage of port `index`
  * (Voltage_out, fdtd_solver.f90:8241-8243), kind 1 / 2 = reflected /
  * transmitted plane sums (:7005-7103; TE for kmax), kind 3 / 4 = their
- * kmax TM sums (:7105-7190).  Steps first_step .. first_step+n-1
- * (1-based); im may be NULL.  Synchronises the handle's stream. */
+ * kmax TM sums (:7105-7190), kind 6 = point probe (extension `probe i j k`;
+ * index 3 p + c for probe p and component c = Ex, Ey, Ez, each the
+ * cell-centred average of the phase-centre sample, :8273-8275).  Steps
+ * first_step .. first_step+n-1 (1-based); im may be NULL.  Synchronises the
+ * handle's stream. */
 int aem_read_probe(aem_handle* h, int kind, int index, int first_step, int n, double* re, double* im);
 
 /* On-the-fly spectrum of a per-step series (the run's sidecar extension
@@ -202,7 +215,9 @@ int aem_dft_batch(const double* x, long long ld, int nseries, long long n, doubl
  * present on every GPU that loads the library until the process exits,
  * which bounds nf to 65536 frequencies: larger nf fails with AEM_ERR_ARG.
  * The first call on each device looks up that array's device address (with
- * the device current); make that first call before any stream capture.
+ * the device current) and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not call this entry point on
+ * a device after cudaDeviceReset (the kept address may be stale).
  * All calls share the array: calls that may overlap on the GPU (different
  * streams, or different threads) race and must be serialised by the
  * caller.  This entry point has no counterpart in the reference. */

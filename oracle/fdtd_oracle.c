@@ -205,6 +205,7 @@ static const real_t mu_0 = R(1.25663706E-6);
 static const real_t ep_0 = R(8.85418782E-12);
 static const real_t pi = R(3.14159265358979323846);
 static const int m_pml = 3, ma_pml = 1;
+static int cpml_m = 3; /* grading order of the CPML tables (sidecar cpml_grading) */
 
 static real_t spread, t_spread, del_t, min_steps;
 static real_t del_x, del_y, del_z;
@@ -401,6 +402,7 @@ int main(int argc, char **argv) {
         printf("Post processing some data...\n");
         finalize_and_write();
     }
+    dump_series_if_requested(max_steps);
     dump_fields_if_requested();
     return 0;
 }

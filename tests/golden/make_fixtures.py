@@ -1,7 +1,7 @@
 """Regenerate the committed golden fixtures from the reference checkout.
 
-Run in a container that has the AlpineEM reference at ``--ref`` (default
-``/root/reference``):
+Run in a container that has the AlpineEM reference at ``--ref`` (default:
+the ALPINEEM_REFERENCE environment variable, else ``/root/reference``):
 
     python tests/golden/make_fixtures.py
 
@@ -120,7 +120,7 @@ def _thin_csv(src, dst, stride):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ALPINEEM_REFERENCE", "/root/reference"))
     ap.add_argument("--stride", type=int, default=4)
     args = ap.parse_args()
     manifest = {}

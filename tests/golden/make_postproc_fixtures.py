@@ -34,7 +34,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
-REF = "/root/reference/examples"
+# the reference checkout whose example post-processors this script runs
+REF = os.path.join(os.environ.get("ALPINEEM_REFERENCE", "/root/reference"), "examples")
 ORACLE = os.path.join(ROOT, "oracle", "_build", "fdtd_oracle")
 ORACLE_K = os.path.join(ROOT, "oracle", "_build", "fdtd_oracle_kmax")
 KMAX_EX = "oblique_angle_plane_waves_w_periodic_boundaries_kmax"

@@ -84,3 +84,60 @@ def test_checkpoint_rejects_other_files(tmp_path, gpu_lib):
             sim.checkpoint_load(str(tmp_path / "missing.ckpt"))
         sim.run(2)
         assert sim.steps[0] == 2
+
+
+def test_truncated_checkpoint_leaves_the_handle_unchanged(tmp_path, gpu_lib):
+    """A truncated file is rejected before any buffer is overwritten: the
+    handle keeps its own state and step count and runs on as if the load
+    had not been tried."""
+    import alpineem_b200 as ab
+    a, b, c = tmp_path / "a", tmp_path / "b", tmp_path / "c"
+    for p in (a, b, c):
+        p.mkdir()
+    ck = tmp_path / "state.ckpt"
+    sim, _ = _sim("dipole_port", a)
+    with sim:
+        sim.run(20)
+        sim.checkpoint_save(str(ck))
+    data = ck.read_bytes()
+    short = tmp_path / "short.ckpt"
+    short.write_bytes(data[:len(data) - 100])
+    sim, _ = _sim("dipole_port", b)
+    with sim:
+        sim.run(7)
+        with pytest.raises(ab.AemError, match="truncated"):
+            sim.checkpoint_load(str(short))
+        assert sim.steps[0] == 7
+        sim.run(13)
+        got = [sim.field(f) for f in FIELDS]
+    sim, _ = _sim("dipole_port", c)
+    with sim:
+        sim.run(20)
+        want = [sim.field(f) for f in FIELDS]
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+
+
+def test_checkpoint_does_not_depend_on_the_watchdog(tmp_path, gpu_lib):
+    """The watchdog's flag is scratch, not run state: a checkpoint written
+    with `watchdog K` on loads into a handle of the same deck without it,
+    and the reverse, and both continue to the same fields."""
+    import alpineem_b200 as ab
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    decks.write_deck("dipole_port", str(a))
+    decks.write_deck("dipole_port", str(b))
+    (a / "inputs.txt.b200").write_text("watchdog 10\n")
+    ck_w, ck_n = str(tmp_path / "w.ckpt"), str(tmp_path / "n.ckpt")
+    with ab.Simulation(str(a / "inputs.txt"), outdir=str(a)) as sw, ab.Simulation(str(b / "inputs.txt"), outdir=str(b)) as sn:
+        sw.run(11)
+        sn.run(11)
+        sw.checkpoint_save(ck_w)
+        sn.checkpoint_save(ck_n)
+        sw.checkpoint_load(ck_n)
+        sn.checkpoint_load(ck_w)
+        sw.run(20)
+        sn.run(20)
+        for f in FIELDS:
+            assert np.array_equal(sw.field(f), sn.field(f))

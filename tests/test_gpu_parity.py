@@ -25,11 +25,17 @@ TOL = 1e-4
 pytestmark = pytest.mark.gpu
 
 
-def _run_oracle(binary, d, max_steps=None):
-    env = dict(os.environ, ORACLE_DUMP=os.path.join(d, "fields.bin"))
+def _run_oracle(binary, d, max_steps=None, dump_fields=True, dump_series=False):
+    """Run the oracle on d/inputs.txt; optionally dump the final fields
+    (ORACLE_DUMP) and the raw plane-sum series (ORACLE_SERIES_DIR)."""
+    env = dict(os.environ)
+    if dump_fields:
+        env["ORACLE_DUMP"] = os.path.join(d, "fields.bin")
+    if dump_series:
+        env["ORACLE_SERIES_DIR"] = d
     if max_steps:
         env["ORACLE_MAX_STEPS"] = str(max_steps)
-    r = subprocess.run([binary, "inputs.txt"], cwd=d, env=env, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([binary, "inputs.txt"], cwd=d, env=env, capture_output=True, text=True, timeout=1800)
     assert r.returncode == 0, r.stdout + r.stderr
 
 
