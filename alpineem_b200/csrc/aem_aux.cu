@@ -232,11 +232,26 @@ __global__ void k_ff_currents(const __grid_constant__ AemParams P, const __grid_
             v[3] = (-1.0f * sg) * ((fget<T>(P, Hx, i, j, k) + fget<T>(P, Hx, i + 1, j, k)) / 2.0f) * w;
         }
         T* cur = reinterpret_cast<T*>(F.cur[a][s]);
-        T* dif = reinterpret_cast<T*>(F.dbuf[a][s]);
         const long long n = F.face_n[a];
+        if constexpr (sizeof(T) == sizeof(float)) {
+            if (F.dtile) {
+                // tiled difference buffer of the batched binning: tile of
+                // (u, v), slot `slot` (1-based step of the batch)
+                const int u = (int)(q % nb), vv = (int)(q / nb);
+                const long long tile = F.tile0[2 * a + s] + (u >> 5) + (long long)(vv >> 5) * F.tiles_u[a];
+                float* dt = F.dtile + (tile * FF_SLOTS + slot) * 4 * 1024 + ((vv & 31) << 5) + (u & 31);
+                for (int m = 0; m < 4; m++) {
+                    const float nv = v[m];
+                    dt[m * 1024] = nv - cur[m * n + q];  // M - M_o, ref :7667
+                    cur[m * n + q] = nv;
+                }
+                continue;
+            }
+        }
+        T* dif = reinterpret_cast<T*>(F.dbuf[a][s]);
         for (int m = 0; m < 4; m++) {
             const T nv = unphase<T>(P, F, v[m], i, j, k, a);
-            dif[((long long)m * F.tb + slot) * n + q] = nv - cur[m * n + q];  // M - M_o, ref :7667
+            dif[(long long)m * n + q] = nv - cur[m * n + q];  // M - M_o, ref :7667
             cur[m * n + q] = nv;
         }
     }
@@ -274,7 +289,7 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
         const T* dif = reinterpret_cast<const T*>(F.dbuf[a][s]);
         const long long n = F.face_n[a];
         T d[4];
-        for (int m = 0; m < 4; m++) d[m] = dif[(long long)m * F.tb * n + q];  // slot 0
+        for (int m = 0; m < 4; m++) d[m] = dif[(long long)m * n + q];
         // component slots: W = 0..2, U = 3..5; (M1, M2, J1, J2) per face normal
         const int u1 = a == 0 ? 4 : 3, u2 = a == 2 ? 4 : 5, w1 = a == 0 ? 1 : 0, w2 = a == 2 ? 1 : 2;
         const float* A = F.ang + 4 * ang;  // sin(th), cos(th), sin(ph), cos(ph)
@@ -308,197 +323,6 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
             atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[3] * sm[3]));
             atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii], wt * fac * (d[3] * sm[3]));
         }
-    }
-}
-
-// Time-batched retarded-time binning (FP32 fields).  The contribution of face
-// cell c at step n to angle g is the reference's (ref :7667-7730)
-//   t = n + 1/2 + tf(c,g) - 1 (U, from M)   or   n + tf(c,g) - 1 (W, from J),
-//   U(ii) += (1-w) fac dM,  U(ii+1) += w fac dM,  ii = int(t), w = t - ii,
-// with tf(c,g) = K0 + Ku*u + Kv*v fixed over the run ((u, v): the face's cell
-// indices; host-precomputed per angle and face).  The differences of F.tb
-// steps are kept (F.dbuf) and binned here in one pass.  A CTA takes one
-// 32x32 tile of one face and a group of virtual angles (angle, image pass)
-// whose delay changes more slowly along one face axis ("walk axis"; the host
-// groups the angles of each face by it).  Lane t of each warp owns step
-// n0+t and holds the differences of an 8-cell strip along the walk axis in
-// registers.  For every angle the lane walks the strip in the direction of
-// increasing delay, summing the two interpolation weights in registers while
-// the bin stays the same; when the bin advances by one, the finished low bin
-// goes to a shared histogram and the high-bin sum carries over as the next
-// run's low-bin sum (both weights of the same bin).  Lanes own distinct bins,
-// so the shared atomics never collide within an instruction.  Each histogram
-// goes to U/W once per batch, one global atomic per non-zero bin, scaled by
-// fac and the image-pass sign.
-constexpr int FF_STRIP = 8;
-// add (a, b) to a shared (U1, U2) or (W1, W2) bin pair with one 64-bit
-// compare-and-swap (a float atomic add to shared memory is such a loop per
-// value; the two components of a pair always share their bin)
-__device__ __forceinline__ void hadd2(float2* p, float a, float b) {
-    unsigned long long* q = reinterpret_cast<unsigned long long*>(p);
-    unsigned long long old = *q, assumed;
-    do {
-        assumed = old;
-        const float x = __uint_as_float((unsigned)assumed) + a;
-        const float y = __uint_as_float((unsigned)(assumed >> 32)) + b;
-        old = atomicCAS(q, assumed, (unsigned long long)__float_as_uint(x) | ((unsigned long long)__float_as_uint(y) << 32));
-    } while (old != assumed);
-}
-// one lane's walk over a strip for one angle, in increasing delay (REV:
-// from the strip's end); see k_ff_bin_batch
-template <bool REV>
-__device__ __forceinline__ void ff_walk(const float (&d)[FF_STRIP][4], float kw, float tf0, int w0, float fn, float fnh,
-                                        float2* hist, int oU, int oW, int lo_ok, int hi_ok, int& bad) {
-    int kU = INT_MIN, kW = INT_MIN;
-    float u1l = 0.0f, u1h = 0.0f, u2l = 0.0f, u2h = 0.0f, w1l = 0.0f, w1h = 0.0f, w2l = 0.0f, w2h = 0.0f;
-#pragma unroll
-    for (int jj = 0; jj < FF_STRIP; jj++) {
-        const int j = REV ? FF_STRIP - 1 - jj : jj;
-        const float tf = fmaf(kw, (float)(w0 + j), tf0);
-        const float tu = (fnh + tf) - 1.0f;
-        const int iu = (int)tu;
-        const float wu = tu - (float)iu;
-        const float tw = (fn + tf) - 1.0f;
-        const int iw = (int)tw;
-        const float ww = tw - (float)iw;
-        if (iu != kU) {
-            if (kU != INT_MIN) {
-                if (kU >= lo_ok && kU <= hi_ok) {
-                    hadd2(&hist[oU + kU - 1], u1l, u2l);
-                    if (iu == kU + 1) {  // the high bin continues as the next low bin
-                        u1l = u1h; u2l = u2h;
-                    } else {
-                        hadd2(&hist[oU + kU], u1h, u2h);
-                        u1l = u2l = 0.0f;
-                    }
-                } else {
-                    bad++;
-                    u1l = u2l = 0.0f;
-                }
-            }
-            kU = iu; u1h = u2h = 0.0f;
-        }
-        if (iw != kW) {
-            if (kW != INT_MIN) {
-                if (kW >= lo_ok && kW <= hi_ok) {
-                    hadd2(&hist[oW + kW - 1], w1l, w2l);
-                    if (iw == kW + 1) {
-                        w1l = w1h; w2l = w2h;
-                    } else {
-                        hadd2(&hist[oW + kW], w1h, w2h);
-                        w1l = w2l = 0.0f;
-                    }
-                } else {
-                    bad++;
-                    w1l = w2l = 0.0f;
-                }
-            }
-            kW = iw; w1h = w2h = 0.0f;
-        }
-        u1l = fmaf(1.0f - wu, d[j][0], u1l); u1h = fmaf(wu, d[j][0], u1h);
-        u2l = fmaf(1.0f - wu, d[j][1], u2l); u2h = fmaf(wu, d[j][1], u2h);
-        w1l = fmaf(1.0f - ww, d[j][2], w1l); w1h = fmaf(ww, d[j][2], w1h);
-        w2l = fmaf(1.0f - ww, d[j][3], w2l); w2h = fmaf(ww, d[j][3], w2h);
-    }
-    if (kU >= lo_ok && kU <= hi_ok) {
-        hadd2(&hist[oU + kU - 1], u1l, u2l);
-        hadd2(&hist[oU + kU], u1h, u2h);
-    } else bad++;
-    if (kW >= lo_ok && kW <= hi_ok) {
-        hadd2(&hist[oW + kW - 1], w1l, w2l);
-        hadd2(&hist[oW + kW], w1h, w2h);
-    } else bad++;
-}
-
-__global__ void __launch_bounds__(256, 3) k_ff_bin_batch(const __grid_constant__ AemParams P,
-                                                         const __grid_constant__ FarFieldDev F, int n0, int nt) {
-    if (P.dstep) n0 = *P.dstep - nt + 1;  // graph replay: the batch ends at the current step
-    extern __shared__ float hist[];  // [group][U, W][hspan][2]: (U1, U2) and (W1, W2) pairs per bin
-    float2* hist2 = reinterpret_cast<float2*>(hist);
-    __shared__ float ksh[64][3];
-    __shared__ int bsh[64], vash[64];
-    const int G = F.group, HS = F.hspan;
-    // face (a, s) of this tile
-    const long long tile = blockIdx.x;
-    int f = 0;
-    while (f < 5 && tile >= F.tile0[f + 1]) f++;
-    const int* grp = F.grp + ((long long)f * F.ngrp + blockIdx.y) * 3;
-    const int walk_v = grp[0], first = grp[1], ng = grp[2];
-    if (ng == 0) return;  // uniform over the CTA
-    const int a = f >> 1, s = f & 1;
-    const long long tl = tile - F.tile0[f];
-    const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
-    const int nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
-    const int u0 = (int)(tl % F.tiles_u[a]) * FF_TILE, v0 = (int)(tl / F.tiles_u[a]) * FF_TILE;
-    const long long n = F.face_n[a];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    for (int e = tid; e < G * 4 * HS; e += blockDim.x) hist[e] = 0.0f;
-    if (tid < ng) {
-        const int va = F.alist[(long long)f * F.nvang + first + tid];
-        vash[tid] = va;
-        const float* k = F.kf + (((long long)va * 3 + a) * 2 + s) * 3;
-        ksh[tid][0] = k[0]; ksh[tid][1] = k[1]; ksh[tid][2] = k[2];
-        // lowest bin any contribution of the tile can reach, less a margin
-        const float tmin = k[0] + k[1] * (float)(k[1] < 0.0f ? u0 + FF_TILE - 1 : u0) +
-                           k[2] * (float)(k[2] < 0.0f ? v0 + FF_TILE - 1 : v0);
-        bsh[tid] = (int)floorf((float)n0 + tmin - 1.0f) - 3;
-    }
-    __syncthreads();
-
-    const float fn = (float)(n0 + lane), fnh = fn + 0.5f;
-    const bool live = lane < nt;
-    const float* dif = reinterpret_cast<const float*>(F.dbuf[a][s]);
-    int bad = 0;
-    constexpr int STRIPS = FF_TILE * (FF_TILE / FF_STRIP);  // 128 strips per tile
-    for (int sid = warp; sid < STRIPS; sid += 8) {
-        // strip start (u, v) and step along the walk axis
-        const int across = sid / (FF_TILE / FF_STRIP), along = (sid % (FF_TILE / FF_STRIP)) * FF_STRIP;
-        const int us = walk_v ? u0 + across : u0 + along;
-        const int vs = walk_v ? v0 + along : v0 + across;
-        if (us >= nb || vs >= nc) continue;  // warp-uniform
-        float d[FF_STRIP][4];
-#pragma unroll
-        for (int j = 0; j < FF_STRIP; j++) {
-            const int u = walk_v ? us : us + j, v = walk_v ? vs + j : vs;
-            const bool ok = live && u < nb && v < nc;
-            const long long q = (long long)v * nb + u;
-#pragma unroll
-            for (int m = 0; m < 4; m++) d[j][m] = ok ? __ldg(dif + ((long long)m * F.tb + lane) * n + q) : 0.0f;
-        }
-        for (int g = 0; g < ng; g++) {
-            const float K0 = ksh[g][0], Ku = ksh[g][1], Kv = ksh[g][2];
-            const float kw = walk_v ? Kv : Ku;
-            const float tf0 = walk_v ? fmaf(Ku, (float)us, K0) : fmaf(Kv, (float)vs, K0);
-            const int w0 = walk_v ? vs : us;
-            // histogram offsets: the U pair of bin k of angle g is hist2[2g HS + k - bsh[g]],
-            // the W pair HS pairs further
-            const int oU = g * 2 * HS - bsh[g], oW = oU + HS;
-            const int lo_ok = bsh[g] + 1, hi_ok = bsh[g] + HS - 1;
-            if (kw >= 0.0f)
-                ff_walk<false>(d, kw, tf0, w0, fn, fnh, hist2, oU, oW, lo_ok, hi_ok, bad);
-            else
-                ff_walk<true>(d, kw, tf0, w0, fn, fnh, hist2, oU, oW, lo_ok, hi_ok, bad);
-        }
-    }
-    if (bad) atomicAdd(F.err, bad);
-    __syncthreads();
-
-    // histogram -> U/W; component slots (W = 0..2, U = 3..5) of (M1, M2, J1, J2)
-    const int mc1 = b, mc2 = c;  // tangential axes
-    float* UW = reinterpret_cast<float*>(F.UW);
-    for (int e = tid; e < ng * 4 * HS; e += blockDim.x) {
-        const float h = hist[e];
-        if (h == 0.0f) continue;
-        // e = ((g * 2 + half) * HS + k) * 2 + comp; m = 0 U1, 1 U2, 2 W1, 3 W2
-        const int g = e / (4 * HS), r = e % (4 * HS), m = (r / (2 * HS)) * 2 + (r & 1), k = (r % (2 * HS)) >> 1;
-        const int va = vash[g], ang = va % F.nang, pass = va / F.nang;
-        const long long gi = (long long)bsh[g] + k;
-        if (gi < 0 || gi >= F.len) { atomicAdd(F.err, 1); continue; }
-        float sg = 1.0f;
-        if (pass) sg = m == 0 ? F.M_mir[mc1] : m == 1 ? F.M_mir[mc2] : m == 2 ? F.J_mir[mc1] : F.J_mir[mc2];
-        const int slotc = m == 0 ? (a == 0 ? 4 : 3) : m == 1 ? (a == 2 ? 4 : 5) : m == 2 ? (a == 0 ? 1 : 0) : (a == 2 ? 1 : 2);
-        atomicAdd(&UW[((long long)slotc * F.nang + ang) * F.len + gi], h * F.fac[a] * sg);
     }
 }
 
@@ -714,24 +538,14 @@ int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaS
     return 1;
 }
 int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s) {
-    if (!F.nang) return 0;
+    // per-step binning with float atomics: the constant-k (complex) path;
+    // FP32 runs use the tiled batch binning of aem_ffbin.cu
+    if (!F.nang || !P.kmax) return 0;
     long long tot = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]) * F.nang;
     if (tot == 0) return 0;
     int blocks = (int)((tot + 255) / 256 < 148 * 32 ? (tot + 255) / 256 : 148 * 32);
-    if (P.kmax) k_ff_bin<cf><<<blocks, 256, 0, s>>>(P, F, counter);
-    else k_ff_bin<float><<<blocks, 256, 0, s>>>(P, F, counter);
+    k_ff_bin<cf><<<blocks, 256, 0, s>>>(P, F, counter);
     return 1;
-}
-size_t ff_batch_smem(const FarFieldDev& F) { return (size_t)F.group * 4 * F.hspan * sizeof(float); }
-int launch_ff_bin_batch(const AemParams& P, const FarFieldDev& F, int n0, int nt, cudaStream_t s) {
-    if (!F.nang || nt <= 0 || F.tile0[6] == 0) return 0;
-    dim3 grid((unsigned)F.tile0[6], (unsigned)F.ngrp);
-    k_ff_bin_batch<<<grid, 256, ff_batch_smem(F), s>>>(P, F, n0, nt);
-    return 1;
-}
-void ff_batch_prepare() {
-    // the histograms may exceed the 48 KB default of dynamic shared memory
-    cudaFuncSetAttribute(k_ff_bin_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 int launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {
     int n = 0;

@@ -33,11 +33,16 @@ using cplx = std::complex<float>;
 // operation order: Wt = (wx c1) c2 + (wy c1) s2 - wz s1, Wp = (-1 wx) s2 +
 // wy c2 (U likewise), Et = (-1 eta) Wt - Up, Ep = (-1 eta) Wp + Ut.  The
 // angle's cosines and sines come from the host.
-template <typename V>
-__device__ inline void ff_pol(const V* uw, long long stride, long long j, const float* cs, float eta, V& Et, V& Ep) {
+// The accumulators A are FP64 on the FP32 path (rounded to FP32 here, the
+// precision the reference's U/W arrays hold) and complex64 for kmax.
+__device__ inline float to_v(double x, float) { return (float)x; }
+__device__ inline cf to_v(cf x, cf) { return x; }
+template <typename V, typename A>
+__device__ inline void ff_pol(const A* uw, long long stride, long long j, const float* cs, float eta, V& Et, V& Ep) {
     const float c1 = cs[0], s1 = cs[1], c2 = cs[2], s2 = cs[3];
-    const V wx = uw[j], wy = uw[stride + j], wz = uw[2 * stride + j];
-    const V ux = uw[3 * stride + j], uy = uw[4 * stride + j], uz = uw[5 * stride + j];
+    const V z{};
+    const V wx = to_v(uw[j], z), wy = to_v(uw[stride + j], z), wz = to_v(uw[2 * stride + j], z);
+    const V ux = to_v(uw[3 * stride + j], z), uy = to_v(uw[4 * stride + j], z), uz = to_v(uw[5 * stride + j], z);
     const V Wt = wx * c1 * c2 + wy * c1 * s2 - wz * s1;
     const V Wp = -1.0f * wx * s2 + wy * c2;
     const V Ut = ux * c1 * c2 + uy * c1 * s2 - uz * s1;
@@ -53,11 +58,11 @@ __device__ inline bool nz(cf v) { return v.x != 0.0f || v.y != 0.0f; }
 // give the output window start o (ref :8520-8530), then the T values from o
 // are written.  UW rows: [component][angle][L]; an angle whose delays equal
 // an earlier one's reads that angle's rows (canon).
-template <typename V>
-__global__ void k_ff_out(const V* UW, int nff, long long L, int len_ff, int T, const float* trig, float eta,
+template <typename V, typename A>
+__global__ void k_ff_out(const A* UW, int nff, long long L, int len_ff, int T, const float* trig, float eta,
                          const int* canon, V* eth, V* eph, int* out_time) {
     const int i = blockIdx.x;
-    const V* uw = UW + (long long)canon[i] * L;
+    const A* uw = UW + (long long)canon[i] * L;
     const long long stride = (long long)nff * L;
     const float* cs = trig + 4 * i;
     __shared__ int first[2];
@@ -122,6 +127,7 @@ void Solver::finalize_and_write() {
     const bool K = d.kmax;
     const int T = d.steps;
     flush_farfield(done_);
+    flush_farfield_tail();
     full_flush();
     AEM_CUDA(cudaStreamSynchronize(stream_));
     const float mu0 = 1.25663706E-6f, ep0 = 8.85418782E-12f, c0 = 299792458.0f, pi = 3.14159265358979323846f;
@@ -129,7 +135,7 @@ void Solver::finalize_and_write() {
         int err = 0;
         AEM_CUDA(cudaMemcpy(&err, FF_.err, sizeof err, cudaMemcpyDeviceToHost));
         d2h_bytes_ += sizeof err;
-        if (err) throw std::runtime_error("far-field binning: " + std::to_string(err) + " contributions outside their histogram");
+        if (err) throw std::runtime_error("far-field binning: " + std::to_string(err) + " contributions outside their window");
     }
     if (P_.err) {
         int err = 0;
@@ -212,11 +218,11 @@ void Solver::finalize_and_write() {
         AEM_CUDA(cudaMemcpyAsync(d_trig, trig.data(), trig.size() * sizeof(float), cudaMemcpyHostToDevice, stream_));
         AEM_CUDA(cudaMemcpyAsync(d_canon, canon.data(), canon.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
         if (K)
-            k_ff_out<cf><<<nff, 256, 0, stream_>>>((const cf*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta, d_canon,
-                                                   (cf*)d_eth, (cf*)d_eph, d_time);
+            k_ff_out<cf, cf><<<nff, 256, 0, stream_>>>((const cf*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta,
+                                                       d_canon, (cf*)d_eth, (cf*)d_eph, d_time);
         else
-            k_ff_out<float><<<nff, 256, 0, stream_>>>((const float*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta,
-                                                      d_canon, (float*)d_eth, (float*)d_eph, d_time);
+            k_ff_out<float, double><<<nff, 256, 0, stream_>>>((const double*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig,
+                                                              eta, d_canon, (float*)d_eth, (float*)d_eph, d_time);
         AEM_CUDA(cudaGetLastError());
         AEM_CUDA(cudaMemcpyAsync(data_out_time.data(), d_time, nff * sizeof(int), cudaMemcpyDeviceToHost, stream_));
         d2h_bytes_ += nff * sizeof(int);

@@ -41,28 +41,42 @@ struct FarFieldDev {
     float wall_lo[3], wall_hi[3];
     const float* ang;           // per angle: sin(th), cos(th), sin(ph), cos(ph)
     void* cur[3][2];            // per face normal / side: the 4 current components of the last step
-    void* dbuf[3][2];           // per face: (new - old) of the 4 components, [comp][slot][cell], tb slots
+    void* dbuf[3][2];           // per face (constant-k path): (new - old) of the 4 components, [comp][cell]
     long long face_n[3];        // cells per face of that normal
-    void* UW;                   // [6][nang][len]: Wx,Wy,Wz,Ux,Uy,Uz
+    void* UW;                   // [6][nang][len]: Wx,Wy,Wz,Ux,Uy,Uz (FP64 sums on the FP32 path, complex64 for kmax)
     int mirror;                 // image-ground-plane pass
     float mir_off[3], use_mir[3], M_mir[3], J_mir[3];
     float kc3[3];               // kmax: k_count for Bloch-phase removal
-    // time-batched binning (FP32 path): tb steps of differences are kept and
-    // binned together; tb == 1 bins every step with the per-contribution kernel
+    // time-batched binning (FP32 path): the differences of tb steps are kept
+    // and binned together; tb == 1 (constant-k runs) bins every step with
+    // the per-contribution kernel and float atomics
     int tb;
     int nvang;                  // virtual angles: nang * (1 + mirror), image pass second
-    int hspan, group;           // histogram bins per (angle, component); angles per CTA
     int tiles_u[3], tiles_v[3]; // 32x32 tiles per face of each normal
     long long tile0[7];         // first tile of face (a, s) at index 2a+s
+    int ntiles;                 // tiles over all six faces (tile0[6])
     const float* kf;            // [nvang][3][2][3]: K0, Ku, Kv of the retarded-time offset tf(u, v)
-    const int* alist;           // [6 faces][nvang]: virtual angles, those walked along u first
-    const int* grp;             // [6 faces][ngrp][3]: walk along v?, first alist entry, count (0 = none)
-    int ngrp;                   // angle groups per face (grid y of the batch kernel)
-    int* err;                   // count of contributions that fell outside a histogram (must stay 0)
+    // deterministic tiled binning (FP32 path, aem_ffbin.cu)
+    float* dtile;               // [tile][FF_SLOTS][4][1024] current differences; slot 0: the step before the batch
+    int nvc;                    // binned (canonical) virtual angles
+    const int* vlist;           // [nvc] their virtual-angle ids
+    int hs;                     // bins of one (tile, angle) window (lanes included)
+    int group;                  // angles per binning CTA (a multiple of the warps)
+    int ngrp;                   // angle groups: ceil(nvc / group)
+    const int* kb;              // [tile][nvc] window base: the lowest bin offset any cell of the tile reaches
+    float* part;                // [tile][nvc][4][hs] window sums of one batch (U1, U2, W1, W2)
+    const int* srt;             // [nvc][6][maxt] tiles of each face sorted by (kb, tile)
+    const int* srtkb;           // the same layout: kb of each sorted tile
+    int maxt;                   // tiles of the largest face
+    int nangc;                  // canonical angles (reduction CTAs)
+    const int* clist;           // [nangc][4]: angle, j of pass 0, j of pass 1 (-1: none), unused
+    const int* crange;          // [nangc][2]: bin offsets [lo, hi) the angle's windows cover
+    int* err;                   // count of contributions that fell outside a window (must stay 0)
 };
 
-constexpr int FF_TB = 32;    // steps per far-field batch (one per warp lane)
-constexpr int FF_TILE = 32;  // face tile edge of the batched binning
+constexpr int FF_TB = 32;     // steps per far-field batch (one per warp lane)
+constexpr int FF_TILE = 32;   // face tile edge of the batched binning
+constexpr int FF_SLOTS = 34;  // difference slots per tile: carry, 32 steps, one spare
 
 // per-step output taps
 struct TapDev {
@@ -107,9 +121,15 @@ int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStrea
 int launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
 int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaStream_t s);
 int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s);
-int launch_ff_bin_batch(const AemParams& P, const FarFieldDev& F, int n0, int nt, cudaStream_t s);
-size_t ff_batch_smem(const FarFieldDev& F);  // dynamic shared bytes of one batch CTA
-void ff_batch_prepare();                     // raise the kernel's shared-memory limit (once per device)
+// deterministic tiled binning (aem_ffbin.cu): bin `nlanes` steps starting at
+// n0 (the differences in slots 1..nlanes, the step before in slot 0), add
+// the windows to the FP64 accumulators in a fixed order, then move slot
+// `carry` to slot 0 for the next batch (carry < 0: no move)
+int launch_ff_bin_tiles(const AemParams& P, const FarFieldDev& F, int n0, int nlanes, int carry, cudaStream_t s);
+// window bases kb and the largest window span over all (tile, angle)
+int launch_ff_base(const FarFieldDev& F, int* kb, int* span, cudaStream_t s);
+size_t ff_tiles_smem(const FarFieldDev& F);  // dynamic shared bytes of one binning CTA
+void ff_tiles_prepare();                     // raise the kernel's shared-memory limit (once per device)
 // fused H+E step (aem_yee.cu): usable when the deck has none of TF/SF,
 // sheets, Drude poles, gridded ports, kmax
 bool yee_fused_ok(const AemParams& P, int gridded_ports);

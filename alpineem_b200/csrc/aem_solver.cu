@@ -96,9 +96,11 @@ void Solver::init() {
         setup_fused();
         AEM_CUDA(cudaStreamSynchronize(stream_));
         nstate_ = bufs_.size();
-        // the watchdog flag is scratch, not run state: allocated after the
-        // state buffers so that checkpoints do not depend on the watchdog
+        // scratch, not run state, allocated after the state buffers so that
+        // checkpoints neither hold nor depend on it: the watchdog flag and
+        // the far-field window sums of one batch
         if (m_.d.ext_watchdog > 0) wd_flag_ = (int*)alloc(sizeof(int));
+        if (ff_part_bytes_) FF_.part = (float*)alloc(ff_part_bytes_);
     } catch (...) {
         release();  // a throwing constructor runs no destructor
         throw;
@@ -462,7 +464,9 @@ void Solver::setup_farfield() {
         ang[4 * q + 3] = std::cos(d.ff_phi[q]);
     }
     F.ang = (const float*)upload(ang);
-    F.UW = alloc((size_t)6 * F.nang * F.len * es_);
+    // accumulators: FP64 on the FP32 path (deterministic ordered sums),
+    // complex64 on the constant-k path
+    F.UW = alloc((size_t)6 * F.nang * F.len * (d.kmax ? es_ : sizeof(double)));
     F.err = (int*)alloc(sizeof(int));
 
     // retarded-time offset of face cell (u, v) for virtual angle va (image
@@ -470,7 +474,6 @@ void Solver::setup_farfield() {
     // with pos the cell's reference index (mirrored in the image pass,
     // ref :7958-8230), written as K0 + Ku u + Kv v
     std::vector<float> kf((size_t)F.nvang * 3 * 2 * 3, 0.0f);
-    double span = 0;
     const int ctr[3] = {F.ic, F.jc, F.kc};
     for (int va = 0; va < F.nvang; va++) {
         const int q = va % F.nang, pass = va / F.nang;
@@ -495,7 +498,6 @@ void Solver::setup_farfield() {
                 k[0] = (float)(((double)F.r_relay - proj0) / (double)F.c_dt);
                 k[1] = (float)(-sg[b] * (double)dl[b] * dir[b] / (double)F.c_dt);
                 k[2] = (float)(-sg[c] * (double)dl[c] * dir[c] / (double)F.c_dt);
-                if (F.face_n[a]) span = std::max(span, std::fabs((double)k[1]) * (FF_TILE - 1) + std::fabs((double)k[2]) * (FF_TILE - 1));
             }
         }
     }
@@ -514,47 +516,92 @@ void Solver::setup_farfield() {
             ff_canon_[q] = first.emplace(key, q).first->second;
         }
     }
-    // time batching on the FP32 path when the histograms fit in shared memory
-    F.hspan = (int)std::ceil(span) + FF_TB + 8;
-    // three CTAs per SM (80 registers, at most 72 KB of histograms each):
-    // the binning is latency-bound on its shared-memory adds
-    const size_t smem_max = 72 * 1024;
-    F.group = (int)std::min<size_t>(64, smem_max / ((size_t)4 * F.hspan * sizeof(float)));
-    // (AEM_FF_PER_STEP=1 keeps the per-step binning kernel, for A/B checks)
-    F.tb = (!d.kmax && F.group >= 1 && !getenv_flag("AEM_FF_PER_STEP")) ? FF_TB : 1;
+    // FP32 runs: batches of FF_TB steps, binned deterministically over 32x32
+    // face tiles (aem_ffbin.cu); constant-k runs bin every step
+    F.tb = d.kmax ? 1 : FF_TB;
     if (F.tb > 1) {
-        // per face: angles whose delay changes more slowly along u are
-        // walked along u, the others along v; groups of F.group angles
-        std::vector<int> alist((size_t)6 * F.nvang), glist;
-        std::vector<std::vector<int>> groups(6);
-        int ngrp = 1;
-        for (int f = 0; f < 6; f++) {
-            const int a = f >> 1, s = f & 1;
-            std::vector<int> cu, cv;
-            for (int va = 0; va < F.nvang; va++) {
-                if (ff_canon_[va % F.nang] != va % F.nang) continue;  // binned by its first angle
-                const float* k = &kf[(((size_t)va * 3 + a) * 2 + s) * 3];
-                (std::fabs(k[1]) <= std::fabs(k[2]) ? cu : cv).push_back(va);
-            }
-            size_t pos = (size_t)f * F.nvang;
-            for (int va : cu) alist[pos++] = va;
-            for (int va : cv) alist[pos++] = va;
-            for (size_t g = 0; g < cu.size(); g += F.group)
-                groups[f].insert(groups[f].end(), {0, (int)g, (int)std::min<size_t>(F.group, cu.size() - g)});
-            for (size_t g = 0; g < cv.size(); g += F.group)
-                groups[f].insert(groups[f].end(), {1, (int)(cu.size() + g), (int)std::min<size_t>(F.group, cv.size() - g)});
-            ngrp = std::max(ngrp, (int)groups[f].size() / 3);
-        }
-        glist.assign((size_t)6 * ngrp * 3, 0);
-        for (int f = 0; f < 6; f++)
-            std::copy(groups[f].begin(), groups[f].end(), glist.begin() + (size_t)f * ngrp * 3);
-        F.ngrp = ngrp;
-        F.alist = (const int*)upload(alist);
-        F.grp = (const int*)upload(glist);
         F.kf = (const float*)upload(kf);
         F.tile0[0] = 0;
         for (int f = 0; f < 6; f++) F.tile0[f + 1] = F.tile0[f] + (long long)F.tiles_u[f >> 1] * F.tiles_v[f >> 1];
-        ff_batch_prepare();
+        F.ntiles = (int)F.tile0[6];
+        F.maxt = 0;
+        for (int f = 0; f < 6; f++) F.maxt = std::max(F.maxt, (int)(F.tile0[f + 1] - F.tile0[f]));
+        // binned virtual angles: those of canonical directions; j of each
+        std::vector<int> vlist, jof(F.nvang, -1);
+        for (int va = 0; va < F.nvang; va++)
+            if (ff_canon_[va % F.nang] == va % F.nang) {
+                jof[va] = (int)vlist.size();
+                vlist.push_back(va);
+            }
+        F.nvc = (int)vlist.size();
+        F.vlist = (const int*)upload(vlist);
+        if (F.ntiles > 0 && F.nvc > 0) {
+            // window bases and spans, from the binning kernel's own expressions
+            int* kb_d = (int*)alloc((size_t)F.ntiles * F.nvc * sizeof(int));
+            int* span_d = (int*)alloc(sizeof(int));
+            launch_ff_base(F, kb_d, span_d, stream_);
+            std::vector<int> kb((size_t)F.ntiles * F.nvc);
+            int span = 0;
+            AEM_CUDA(cudaMemcpyAsync(kb.data(), kb_d, kb.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            AEM_CUDA(cudaMemcpyAsync(&span, span_d, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            AEM_CUDA(cudaStreamSynchronize(stream_));
+            AEM_CUDA(cudaGetLastError());
+            F.kb = kb_d;
+            F.hs = span + FF_TB;  // offsets base .. base+span, plus the 32 lanes
+            // angles per CTA: 8 warps x AW, two CTAs per SM
+            const size_t stage = (size_t)2 * FF_TILE * (4 * 33 + 1) * sizeof(float);
+            const size_t per = (size_t)2 * F.hs * 2 * sizeof(float);
+            F.group = 8;
+            if (stage + 32 * per <= 96 * 1024) F.group = 32;
+            else if (stage + 16 * per <= 96 * 1024) F.group = 16;
+            if (stage + F.group * per > 200 * 1024)
+                throw std::runtime_error("far field: a tile's delay span (" + std::to_string(span) +
+                                         " steps) is too wide for the binning windows");
+            F.ngrp = (F.nvc + F.group - 1) / F.group;
+            // per (j, face): tiles sorted by (kb, tile), for the ordered reduction
+            std::vector<int> srt((size_t)F.nvc * 6 * F.maxt, 0), srtkb((size_t)F.nvc * 6 * F.maxt, INT_MAX);
+            std::vector<int> kbmin((size_t)F.nvc, INT_MAX), kbmax((size_t)F.nvc, INT_MIN);
+            std::vector<int> idx;
+            for (int j = 0; j < F.nvc; j++)
+                for (int f = 0; f < 6; f++) {
+                    const int t0 = (int)F.tile0[f], nt = (int)(F.tile0[f + 1] - F.tile0[f]);
+                    idx.resize(nt);
+                    for (int q = 0; q < nt; q++) idx[q] = t0 + q;
+                    std::sort(idx.begin(), idx.end(), [&](int x, int y) {
+                        const int kx = kb[(size_t)x * F.nvc + j], ky = kb[(size_t)y * F.nvc + j];
+                        return kx != ky ? kx < ky : x < y;
+                    });
+                    const size_t o = ((size_t)j * 6 + f) * F.maxt;
+                    for (int q = 0; q < nt; q++) {
+                        srt[o + q] = idx[q];
+                        srtkb[o + q] = kb[(size_t)idx[q] * F.nvc + j];
+                    }
+                    if (nt) {
+                        kbmin[j] = std::min(kbmin[j], srtkb[o]);
+                        kbmax[j] = std::max(kbmax[j], srtkb[o + nt - 1]);
+                    }
+                }
+            F.srt = (const int*)upload(srt);
+            F.srtkb = (const int*)upload(srtkb);
+            // reduction CTAs: the canonical angles, with the j of each pass
+            std::vector<int> clist, crange;
+            for (int q = 0; q < F.nang; q++) {
+                if (ff_canon_[q] != q) continue;
+                const int j0 = jof[q], j1 = F.mirror ? jof[q + F.nang] : -1;
+                int lo = INT_MAX, hi = INT_MIN;
+                for (int j : {j0, j1})
+                    if (j >= 0) { lo = std::min(lo, kbmin[j]); hi = std::max(hi, kbmax[j] + F.hs); }
+                if (lo > hi) lo = hi = 0;
+                clist.insert(clist.end(), {q, j0, j1, 0});
+                crange.insert(crange.end(), {lo, hi});
+            }
+            F.nangc = (int)clist.size() / 4;
+            F.clist = (const int*)upload(clist);
+            F.crange = (const int*)upload(crange);
+            F.dtile = (float*)alloc((size_t)F.ntiles * FF_SLOTS * 4 * 1024 * sizeof(float));
+            ff_part_bytes_ = (size_t)F.ntiles * F.nvc * 4 * F.hs * sizeof(float);
+            ff_tiles_prepare();
+        }
     } else {
         for (int q = 0; q < F.nang; q++) ff_canon_[q] = q;  // the per-step path bins every angle
     }
@@ -562,7 +609,7 @@ void Solver::setup_farfield() {
         for (int s = 0; s < 2; s++)
             if (F.has[a]) {
                 F.cur[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
-                F.dbuf[a][s] = alloc((size_t)F.face_n[a] * 4 * F.tb * es_);
+                if (F.tb == 1) F.dbuf[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
             }
 }
 
@@ -835,8 +882,8 @@ void Solver::step(int counter) {
         phase(AEM_PHASE_PORTS, [&] { return launch_ports_e(P_, PS_, counter, stream_); });
     }
     if (FF_.tb > 1) {
-        // differences go to slot counter - ff_n0_; a full batch is binned at once
-        phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, counter - ff_n0_, stream_); });
+        // differences go to slot counter - ff_n0_ + 1; a full batch is binned at once
+        phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, counter - ff_n0_ + 1, stream_); });
         if (counter - ff_n0_ + 1 == FF_.tb) flush_farfield(counter);
     } else {
         phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, 0, stream_); });
@@ -846,13 +893,25 @@ void Solver::step(int counter) {
     if (full_.f[0]) full_tap(counter);
 }
 
-// bin the steps ff_n0_..last held in the difference buffer
+// bin the steps ff_n0_..last held in the difference buffer; the last one
+// moves to slot 0, where the next batch takes its carried-over part
 void Solver::flush_farfield(int last) {
     if (FF_.tb > 1 && last >= ff_n0_) {
         const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
-        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_batch(P_, FF_, n0, nt, stream_); });
+        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, nt, stream_); });
     }
     ff_n0_ = last + 1;
+}
+
+// after the deck's last step: the carried-over part of that step, binned as
+// a one-step batch whose own differences are zero; ff_n0_ then points past
+// it, so this runs once (a checkpoint carries ff_n0_)
+void Solver::flush_farfield_tail() {
+    const int steps = m_.d.steps;
+    if (FF_.tb > 1 && done_ == steps && ff_n0_ == steps + 1) {
+        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, steps + 1, 1, -1, stream_); });
+        ff_n0_ = steps + 2;
+    }
 }
 
 // every K steps (extension watchdog K): scan the current E and H for a
@@ -879,6 +938,7 @@ void Solver::run(int n) {
     // partial batches wait for more steps (or for flush())
     if (done_ == m_.d.steps) {
         flush_farfield(done_);
+        flush_farfield_tail();
         full_flush();
     }
     AEM_CUDA(cudaGetLastError());

@@ -72,7 +72,10 @@ class Solver {
     size_t h2d_bytes() const { return h2d_bytes_; }
     size_t d2h_bytes() const { return d2h_bytes_; }
     // bin far-field contributions still held in the batch buffer
-    void flush() { flush_farfield(done_); }
+    void flush() {
+        flush_farfield(done_);
+        flush_farfield_tail();
+    }
     // per-phase device time: with profiling on, every launcher is bracketed
     // by CUDA events on the solver's stream; read_profile sums them
     void set_profiling(bool on);
@@ -113,6 +116,7 @@ class Solver {
     void setup_full();
     void step(int counter);
     void flush_farfield(int last);
+    void flush_farfield_tail();
     bool graph_ready(int g) const;  // can a g-step graph chunk start at the next step?
     void full_tap(int counter);
     void full_drain(int b);
@@ -140,6 +144,7 @@ class Solver {
     bool split_ = false;  // bulk / port / CPML passes (a port inside a CPML slab)
     AemParams split_params_[2];
     int ff_n0_ = 1;  // first step held in the far-field difference buffer
+    size_t ff_part_bytes_ = 0;  // far-field window sums of one batch (scratch)
     // far-field angle whose bins angle q copies (q itself unless q is a
     // second angle of the same direction, e.g. a pole at another phi)
     std::vector<int> ff_canon_;

@@ -126,6 +126,38 @@ def _ellipsoids_small():
 DECKS["ellipsoids_small"] = _ellipsoids_small()
 
 
+def _gridded_port():
+    """A gridded (one-way mode) port on a +z face driving the grid, its mode
+    file written alongside: (4, n1+1, n2+1) float32, first index fastest
+    (E1, E2, H1, H2 weights; fdtd_solver.f90:3723-3744)."""
+    import numpy as np
+    n1, n2 = 8, 6
+    a = np.arange(1, n1 + 2)[None, :]
+    b = np.arange(1, n2 + 2)[:, None]
+    prof = (np.sin(np.pi * a / (n1 + 2)) * np.sin(np.pi * b / (n2 + 2))).astype(np.float32)
+    feed = np.zeros((n2 + 1, n1 + 1, 4), np.float32)
+    feed[..., 0] = 40.0 * prof
+    feed[..., 1] = 12.0 * prof * (a - n1 / 2.0) / n1
+    feed[..., 2] = -0.03 * prof * (b - n2 / 2.0) / n2
+    feed[..., 3] = 0.1 * prof
+    return dict(n=(30, 28, 40), steps=250, f="10E9", pulse=1, excitation=("antenna", 1, 0, 1),
+                ff=[(0, 0), (90, 45), (150, 300)], ffc=(15, 14, 20),
+                mats=[("simple", 5, (2, 2, 2), (0.005, 0.005, 0.005))], objects=[("sphere", 5, (15, 14, 28), 4)],
+                ports=[("gridded", "+z", 50, (11, 11, 15), (n1, n2), "feed.bin")],
+                _files={"feed.bin": feed.tobytes()})
+
+
+# a gridded port: the mode projection of H, the H zeroing behind the feed
+# plane and the E overwrite, with far field
+DECKS["gridded_port"] = _gridded_port()
+# constant-k unit cell with far-field angles: Bloch phase removed from the
+# Huygens currents (ref :7202-7331) and binned every step (ref :7333-7507)
+DECKS["kmax_ff"] = dict(kmax=True, n=(36, 10, 10), dl=("0.25E-3", "0.25E-3", "0.25E-3"), steps=300, f="8E9",
+                        bc=(0, 0, 1, 1, 1, 1), excitation=("plane wave", 1, 0, "TE", "+"), k=("300.0", "150.0"),
+                        ff=[(90, 0), (45, 0), (120, 180)], ffc=(18, 5, 5),
+                        mats=[("simple", 5, (4, 4, 4), (0, 0, 0))], objects=[("block", 5, (14, 1, 1), (8, 10, 10))])
+
+
 def write_deck(name, directory, fname="inputs.txt"):
     """Write deck `name` (and its sidecar / bulk geometry file, if any) into
     `directory`; returns (path, kmax)."""
@@ -138,4 +170,7 @@ def write_deck(name, directory, fname="inputs.txt"):
             f.write(d["_ext"])
     if "_bulk" in d:
         d["_bulk"].tofile(os.path.join(directory, d["bulk"]))
+    for fn, data in d.get("_files", {}).items():
+        with open(os.path.join(directory, fn), "wb") as f:
+            f.write(data)
     return path, bool(d.get("kmax"))

@@ -39,7 +39,7 @@ def _run_oracle(binary, d, max_steps=None, dump_fields=True, dump_series=False):
     assert r.returncode == 0, r.stdout + r.stderr
 
 
-def _check_far_field(name, odat, gdat, peak):
+def _check_far_field(name, odat, gdat, peak, tol=TOL):
     """Far-field series on a common time axis.  The reference writes each
     angle's series from its first non-zero bin (fdtd_solver.f90:8483-8534)
     and records that start in the time correction r/c - (start-1) dt, which
@@ -59,6 +59,36 @@ def _check_far_field(name, odat, gdat, peak):
         so, sg = o["ff"][q], g["ff"][q]
         T = len(so)
         # GPU sample n is oracle sample n + s; compare where both windows hold data
+        n0, n1 = max(0, -s), min(T, T - s)
+        assert n1 - n0 >= T // 2, (name, q, s)
+        err = rel_l2(so[n0 + s:n1 + s], sg[n0:n1], floor=1e-3 * peak)
+        assert err <= tol, "%s: far field %d (angle %d) rel L2 %.3g (start shift %d)" % (name, q, a, err, s)
+
+
+def _kmax_far_field(dat):
+    """Constant-k far-field series of a .dat (complex, per angle theta then
+    phi) and the per-angle time corrections."""
+    blocks, _ = dat_blocks(dat)
+    series, corr = [], None
+    for t, b in blocks:
+        if t.startswith("far field rE"):
+            series.append(b[1:, 0] + 1j * b[1:, 1])  # row 0 holds theta, phi
+        elif t.startswith("far field phase correction"):
+            corr = b[:, 0]
+    return series, corr
+
+
+def _check_far_field_kmax(name, odat, gdat, dt, peak):
+    """As _check_far_field, for the complex series of a constant-k run."""
+    so_all, co = _kmax_far_field(odat)
+    sg_all, cg = _kmax_far_field(gdat)
+    assert len(so_all) == len(sg_all) > 0
+    for q, (so, sg) in enumerate(zip(so_all, sg_all)):
+        a = q // 2
+        sh = (co[a] - cg[a]) / dt
+        s = int(round(sh))
+        assert abs(sh - s) < 1e-3 * max(1.0, abs(sh)), (name, a, sh)
+        T = len(so)
         n0, n1 = max(0, -s), min(T, T - s)
         assert n1 - n0 >= T // 2, (name, q, s)
         err = rel_l2(so[n0 + s:n1 + s], sg[n0:n1], floor=1e-3 * peak)
@@ -107,6 +137,9 @@ def test_deck_parity(name, tmp_path, oracle_bin, gpu_lib):
         assert err <= TOL, "%s: block '%s' rel L2 %.3g" % (name, ta, err)
     if not kmax:
         _check_far_field(name, str(od / fname), str(gd / fname), peak)
+    elif decks.DECKS[name].get("ff"):
+        dt = float(olines[4].split()[3])
+        _check_far_field_kmax(name, str(od / fname), str(gd / fname), dt, peak)
 
     ofields = read_oracle_dump(str(md / "fields.bin"), kmax)
     # a component that stays near zero (e.g. Ex of an x-travelling wave) is
