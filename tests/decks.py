@@ -127,23 +127,23 @@ DECKS["ellipsoids_small"] = _ellipsoids_small()
 
 
 def _gridded_port():
-    """A gridded (one-way mode) port on a +z face driving the grid, its mode
-    file written alongside: (4, n1+1, n2+1) float32, first index fastest
-    (E1, E2, H1, H2 weights; fdtd_solver.f90:3723-3744)."""
+    """A gridded (one-way mode) port feeding a parallel-plate line: two PEC
+    plates (sigma = 1e8) 6 cells apart in y, and on the port plane the TEM
+    mode between them, written alongside as the reference's mode file
+    ((4, n1+1, n2+1) float32, first index fastest: E1, E2, H1, H2 weights
+    per point; fdtd_solver.f90:3723-3744): E along y uniform across the gap
+    (1 / gap), H along x (1 / width)."""
     import numpy as np
-    n1, n2 = 8, 6
-    a = np.arange(1, n1 + 2)[None, :]
-    b = np.arange(1, n2 + 2)[:, None]
-    prof = (np.sin(np.pi * a / (n1 + 2)) * np.sin(np.pi * b / (n2 + 2))).astype(np.float32)
+    n1, n2, dl = 8, 6, 1e-3
     feed = np.zeros((n2 + 1, n1 + 1, 4), np.float32)
-    feed[..., 0] = 40.0 * prof
-    feed[..., 1] = 12.0 * prof * (a - n1 / 2.0) / n1
-    feed[..., 2] = -0.03 * prof * (b - n2 / 2.0) / n2
-    feed[..., 3] = 0.1 * prof
+    feed[:n2, :, 1] = 1.0 / (n2 * dl)
+    feed[:n2, :, 2] = 1.0 / (n1 * dl)
     return dict(n=(30, 28, 40), steps=250, f="10E9", pulse=1, excitation=("antenna", 1, 0, 1),
                 ff=[(0, 0), (90, 45), (150, 300)], ffc=(15, 14, 20),
-                mats=[("simple", 5, (2, 2, 2), (0.005, 0.005, 0.005))], objects=[("sphere", 5, (15, 14, 28), 4)],
-                ports=[("gridded", "+z", 50, (11, 11, 15), (n1, n2), "feed.bin")],
+                mats=[("simple", 1, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (2, 2, 2), (0.005, 0.005, 0.005))],
+                objects=[("block", 1, (6, 9, 10), (20, 1, 24)), ("block", 1, (6, 16, 10), (20, 1, 24)),
+                         ("sphere", 5, (15, 12, 30), 3)],
+                ports=[("gridded", "+z", 50, (11, 10, 15), (n1, n2), "feed.bin")],
                 _files={"feed.bin": feed.tobytes()})
 
 
