@@ -52,10 +52,10 @@ namespace aem {
 
 // 15 owned rows + the -y halo row: 16 warps (512 threads) of at most 128
 // registers, one CTA per SM; the warps hide each other's latency
-constexpr int Y4_TX = 128, Y4_TY = 16, Y4_ZC = 64, Y4_NT = 32 * Y4_TY;
-constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;   // E box 136 x 18, x from x0-4, y from y0-1
-constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;   // H box 132 x 17
-constexpr int Y4_IW = Y4_TX + 16, Y4_IR = Y4_TY + 1;  // id box 144 x 17 bytes, x from x0-16
+constexpr int Y4_TX = 128, Y4_TY = 15, Y4_ZC = 64, Y4_NT = 32 * (Y4_TY + 1);
+constexpr int Y4_EW = Y4_TX + 8, Y4_ER = Y4_TY + 2;   // E box 136 x 17, x from x0-4, y from y0-1
+constexpr int Y4_HW = Y4_TX + 4, Y4_HR = Y4_TY + 1;   // H box 132 x 16
+constexpr int Y4_IW = Y4_TX + 16, Y4_IR = Y4_TY + 1;  // id box 144 x 16 bytes, x from x0-16
 // every TMA destination starts on a 128-byte boundary
 constexpr int y4_up128(int b) { return (b + 127) / 128 * 128; }
 constexpr int Y4_EC = y4_up128(Y4_ER * Y4_EW * 4) / 4;  // floats from one E component tile to the next
@@ -67,16 +67,18 @@ constexpr int Y4_LA = 2;
 constexpr int Y4_ES = Y4_LA + 2, Y4_HS = Y4_LA + 1, Y4_IS = Y4_LA + 2, Y4_NB = Y4_LA + 1;
 constexpr int Y4_OFF_H = Y4_ES * 3 * Y4_EC * 4;
 constexpr int Y4_OFF_I = Y4_OFF_H + Y4_HS * 3 * Y4_HC * 4;
-constexpr int Y4_OFF_DZ = Y4_OFF_I + Y4_IS * Y4_IC;
+constexpr int Y4_OFF_HN = Y4_OFF_I + Y4_IS * Y4_IC;
+constexpr int Y4_HN_F = 2 * Y4_HR * Y4_TX;  // H_new hx, hz of rows y0-1..y0+14
+constexpr int Y4_OFF_DZ = Y4_OFF_HN + Y4_HN_F * 4;
 constexpr int Y4_OFF_DX = Y4_OFF_DZ + 2 * Y4_ZC * 4;
-constexpr int Y4_OFF_GAB = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
-constexpr int Y4_OFF_FAIL = Y4_OFF_GAB + AEM_MAX_MATERIALS * 6 * 4;
-constexpr int Y4_OFF_BAR = Y4_OFF_FAIL + 8;
+constexpr int Y4_OFF_XH = Y4_OFF_DX + (2 * Y4_TX + 4) * 4;
+constexpr int Y4_OFF_GAB = Y4_OFF_XH + 2 * Y4_TY * 2 * 4;
+constexpr int Y4_OFF_BAR = Y4_OFF_GAB + AEM_MAX_MATERIALS * 6 * 4;
 constexpr int Y4_SMEM = Y4_OFF_BAR + Y4_NB * 8;
 constexpr unsigned Y4_TX_E = Y4_ER * Y4_EW * 4, Y4_TX_H = Y4_HR * Y4_HW * 4, Y4_TX_I = Y4_IR * Y4_IW;
 constexpr unsigned Y4_TX_STAGE = 3 * Y4_TX_E + 3 * Y4_TX_H + Y4_TX_I;          // E(t+1), H(t), ids(t)
 constexpr unsigned Y4_TX_FIRST = 9 * Y4_TX_E + 6 * Y4_TX_H + 2 * Y4_TX_I;      // E(z0-1..z0+1), H, ids(z0-1..z0)
-static_assert(Y4_OFF_H % 128 == 0 && Y4_OFF_I % 128 == 0 && Y4_OFF_BAR % 8 == 0, "layout");
+static_assert(Y4_OFF_H % 128 == 0 && Y4_OFF_I % 128 == 0 && Y4_OFF_HN % 128 == 0 && Y4_OFF_BAR % 8 == 0, "layout");
 static_assert(Y4_TX_FIRST < (1u << 20), "mbarrier transaction count");
 static_assert(Y4_SMEM <= 227 * 1024, "shared memory per CTA");
 
