@@ -896,7 +896,8 @@ void Solver::step(int counter) {
 // bin the steps ff_n0_..last held in the difference buffer; the last one
 // moves to slot 0, where the next batch takes its carried-over part
 void Solver::flush_farfield(int last) {
-    if (FF_.tb > 1 && last >= ff_n0_) {
+    if (last < ff_n0_) return;  // nothing buffered (and the tail, if done, stays done)
+    if (FF_.tb > 1) {
         const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
         phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, nt, stream_); });
     }

@@ -14,7 +14,8 @@
   128 x 128 x 512 unit cell (eight anisotropic lossy layers, a 2-pole Drude
   layer, a 100 S sheet, 12-cell CPML on z), 600 of its 8000 steps (the
   oracle needs minutes for the whole run): reflected and transmitted plane
-  sums against the FP32 oracle at <= 1e-4 and the FP64 oracle at <= 1e-4,
+  sums against the FP64 oracle at <= 1e-4, and against the FP32 oracle at
+  <= 1e-4 or twice that oracle's own FP64 error, whichever is larger,
   and the on-the-fly spectra at 256 frequencies against a float64 DFT of the
   run's own samples at <= 1e-12.
 
@@ -122,9 +123,15 @@ def test_layered_slab_full_grid(tmp_path, oracle_bin, gpu_lib):
     peak = max(np.linalg.norm(v) for v in o.values())
     errs32 = {k: rel_l2(o[k], g[k], floor=1e-3 * peak) for k in o}
     errs64 = {k: rel_l2(o64s[k], g[k], floor=1e-3 * peak) for k in o}
-    _report({"deck": "layered_slab_128x128x512_%d_steps" % steps, "probe_rel_l2": max(errs64.values())})
-    assert max(errs32.values()) <= TOL, errs32
+    oracle64 = {k: rel_l2(o64s[k], o[k], floor=1e-3 * peak) for k in o}
+    _report({"deck": "layered_slab_128x128x512_%d_steps" % steps, "probe_rel_l2": max(errs64.values()),
+             "fp32_oracle_rel_l2": max(oracle64.values())})
     assert max(errs64.values()) <= TOL, errs64
+    # against the FP32 oracle: within the tolerance, or within twice the FP32
+    # oracle's own error against FP64 (its 16384-term plane sums are
+    # sequential FP32, the GPU's a tree)
+    for k in o:
+        assert errs32[k] <= max(TOL, 2 * oracle64[k]), (k, errs32[k], oracle64[k])
     m = np.arange(steps)
     for k, (f, X) in spectra.items():
         assert len(f) == 256 and f[0] == 1e9 and f[-1] == 3e10
