@@ -108,6 +108,15 @@ DECKS = {
                          objects=[("block", 4, (150, 11, 8), (1, 1, 4)), ("block", 4, (150, 11, 14), (1, 1, 4)),
                                   ("block", 5, (120, 6, 6), (20, 8, 12)), ("sphere", 5, (256, 11, 13), 5)],
                          ports=[("basic", "z", 50, (150, 11, 13), (1, 1, 1))]),
+    # long in x with the port clear of every CPML slab: three 128-cell x
+    # tiles of the TMA-fed fused kernel (-x halo columns recomputed across
+    # the seams at x = 128 and 256), materials across the seams, far field
+    "fused_wide": dict(n=(300, 40, 34), steps=200, f="15E9", pulse=1, excitation=("antenna", 1, 0, 1),
+                       ff=[(90, 0), (45, 120), (150, 250)], ffc=(150, 20, 17),
+                       mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (4, 3, 2), (0.01, 0, 0))],
+                       objects=[("block", 4, (150, 20, 11), (1, 1, 5)), ("block", 4, (150, 20, 18), (1, 1, 5)),
+                                ("block", 5, (120, 14, 12), (20, 10, 12)), ("sphere", 5, (256, 20, 17), 5)],
+                       ports=[("basic", "z", 50, (150, 20, 17), (1, 1, 1))]),
     # the throughput workload at 48^3: bulk-file ellipsoids, 6-cell CPML
     # (sidecar), a 1-cell port and 56 far-field angles
     "ellipsoids_small": "ellipsoids_small",

@@ -14,7 +14,7 @@ import decks
 pytestmark = pytest.mark.gpu
 
 FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
-FUSED = ["dipole_port", "fused_long_x", "ellipsoids_small", "dipole_pbc_x", "fused_long_z"]
+FUSED = ["dipole_port", "fused_wide", "ellipsoids_small", "dipole_pbc_x", "fused_long_z"]
 
 
 def _fields(name, d, monkeypatch, two_kernel, steps):

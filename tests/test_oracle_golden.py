@@ -49,12 +49,12 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def _check(csv, freq, cols, which):
+def _check(csv, freq, cols, which, tol=TOL):
     fref, ref = postproc.csv_complex(csv)
     got = postproc.match_rows(fref, freq, cols)
     for q in which:
         err = _rel(got[q], ref[q])
-        assert err <= TOL, "%s column %d: rel L2 %.3g" % (os.path.basename(csv), q, err)
+        assert err <= tol, "%s column %d: rel L2 %.3g" % (os.path.basename(csv), q, err)
 
 
 @pytest.mark.parametrize("case", ["multilayer_slab", "drude_slab", "subpixel_slab"])
