@@ -182,24 +182,47 @@ __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid
                 dd[m] = x0 - x1;
             }
             const float uf = (float)(u0 + u);
+            // every angle's bins first, then all histogram loads, adds and
+            // stores: the angles' windows never overlap, so the loads of one
+            // angle need not wait for the stores of another
+            int iu[AW], iw[AW];
+            float wu[AW], ww[AW];
+            bool on[AW];
 #pragma unroll
             for (int q = 0; q < AW; q++) {
-                if (warp + BIN_WARPS * q >= ng) break;  // warp-uniform
                 const BinW w = ff_binw(fmaf(Ku[q], uf, trow[q]));
-                const int iu = w.ku - base[q], iw = w.kw - base[q];
-                if ((unsigned)iu > (unsigned)(HS - 32) || (unsigned)iw > (unsigned)(HS - 32)) {
+                iu[q] = w.ku - base[q];
+                iw[q] = w.kw - base[q];
+                wu[q] = w.wu;
+                ww[q] = w.ww;
+                on[q] = warp + BIN_WARPS * q < ng;  // warp-uniform
+                if (on[q] && ((unsigned)iu[q] > (unsigned)(HS - 32) || (unsigned)iw[q] > (unsigned)(HS - 32))) {
                     bad++;  // never: kb and hs come from the same expressions
-                    continue;
+                    on[q] = false;
                 }
+            }
+            float2 pu[AW], pw[AW];
+#pragma unroll
+            for (int q = 0; q < AW; q++) {
+                if (!on[q]) continue;
+                const float2* h = hist + (warp + BIN_WARPS * q) * 2 * HS;
+                pu[q] = h[iu[q] + lane];
+                pw[q] = h[HS + iw[q] + lane];
+            }
+#pragma unroll
+            for (int q = 0; q < AW; q++) {
+                if (!on[q]) continue;
+                pu[q].x += fmaf(wu[q], dd[0], d[0]);
+                pu[q].y += fmaf(wu[q], dd[1], d[1]);
+                pw[q].x += fmaf(ww[q], dd[2], d[2]);
+                pw[q].y += fmaf(ww[q], dd[3], d[3]);
+            }
+#pragma unroll
+            for (int q = 0; q < AW; q++) {
+                if (!on[q]) continue;
                 float2* h = hist + (warp + BIN_WARPS * q) * 2 * HS;
-                float2 pu = h[iu + lane];
-                pu.x += fmaf(w.wu, dd[0], d[0]);
-                pu.y += fmaf(w.wu, dd[1], d[1]);
-                h[iu + lane] = pu;
-                float2 pw = h[HS + iw + lane];
-                pw.x += fmaf(w.ww, dd[2], d[2]);
-                pw.y += fmaf(w.ww, dd[3], d[3]);
-                h[HS + iw + lane] = pw;
+                h[iu[q] + lane] = pu[q];
+                h[HS + iw[q] + lane] = pw[q];
             }
         }
         if (v + 1 < nv) store_row(stage + ((v + 1) & 1) * STAGE_FLOATS, pre);
