@@ -58,6 +58,7 @@ def load_library():
     lib.aem_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(h)]
     lib.aem_run.argtypes = [h, ctypes.c_int]
     lib.aem_run_graph.argtypes = [h, ctypes.c_int, ctypes.c_int]
+    lib.aem_autotune.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.aem_run_batch.argtypes = [ctypes.POINTER(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.aem_steps.argtypes = [h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.aem_synchronize.argtypes = [h]
@@ -277,6 +278,14 @@ class Simulation:
         re, im = np.zeros(n), np.zeros(n)
         self._check(self._lib.aem_read_probe(self._h, k, int(index), int(first), int(n), _dptr(re), _dptr(im)))
         return (re + 1j * im) if self.kmax else re
+
+    def autotune(self, steps_per_candidate=2):
+        """Tune the general update's launch shape on the run's next steps
+        (up to 8 x steps_per_candidate of them; the fields are unchanged).
+        Returns {"update_h": (z planes, rows), "update_e": (z planes, rows)}."""
+        out = (ctypes.c_int * 4)()
+        self._check(self._lib.aem_autotune(self._h, int(steps_per_candidate), out))
+        return {"update_h": (out[0], out[1]), "update_e": (out[2], out[3])}
 
     def checkpoint_save(self, path):
         """Write the whole run state after the steps done so far to `path`."""

@@ -128,6 +128,14 @@ int aem_run(aem_handle* h, int nsteps) {
     });
 }
 
+int aem_autotune(aem_handle* h, int steps_per_candidate, int shape[4]) {
+    if (!h || steps_per_candidate < 0) return fail(h, AEM_ERR_ARG, "bad argument");
+    return guarded(h, [&]() {
+        h->s->autotune(steps_per_candidate, shape);
+        return AEM_OK;
+    });
+}
+
 int aem_run_graph(aem_handle* h, int nsteps, int steps_per_graph) {
     if (!h || nsteps < 0 || steps_per_graph < 1) return fail(h, AEM_ERR_ARG, "bad argument");
     return guarded(h, [&]() {

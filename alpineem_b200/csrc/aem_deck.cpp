@@ -366,6 +366,18 @@ void apply_extensions(Deck& d, const std::string& text) {
             d.ext_cpml_sigma = sf;
             d.ext_cpml_kappa = km;
             d.ext_cpml_alpha = am;
+        } else if (key == "coef_precision") {
+            // coef_precision 32 (reference FP32 arithmetic) or 64 (the
+            // material and CPML tables in FP64 on the GPU)
+            if (val != "32" && val != "64") throw DeckError("extension coef_precision must be 32 or 64");
+            d.ext_coef64 = val == "64";
+        } else if (key == "autotune") {
+            // autotune N: at the first step, time candidate launch shapes of
+            // the two-kernel update for N steps each (8 candidates)
+            char* end = nullptr;
+            long v = std::strtol(val.c_str(), &end, 10);
+            if (*end || v < 0 || v > 1000) throw DeckError("extension autotune must be 0..1000 steps per candidate");
+            d.ext_autotune = (int)v;
         } else if (key == "tfsf_inset") {
             char* end = nullptr;
             long v = std::strtol(val.c_str(), &end, 10);

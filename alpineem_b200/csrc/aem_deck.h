@@ -130,6 +130,8 @@ struct Deck {
     int ext_tfsf_inset = 0;
     std::vector<std::array<int, 3>> ext_probes;
     int cpml_m = 3;                     // grading order used by the CPML tables
+    int ext_autotune = 0;               // autotune N: steps per candidate launch shape (0: off)
+    bool ext_coef64 = false;            // coef_precision 64: coefficient tables in FP64 on the GPU
 };
 
 // Parse an inputs.txt.  `kmax` selects the constant-k periodic grammar

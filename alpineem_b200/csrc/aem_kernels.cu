@@ -50,11 +50,11 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
     return nw;
 }
 
-// z planes per CTA of the two-kernel path: a grid narrow in x and y (a
-// kmax unit cell) still spreads over every SM.  (Fewer planes per CTA make
-// a single narrow run faster but leave concurrent runs of a batch less room
-// to overlap: the batched constant-k sweep lost 10 %.)
-constexpr int UPD_ZCH = 16;
+// z planes per CTA of the two-kernel path (P.zch_h / P.zch_e) and rows per
+// CTA (P.ty_h / P.ty_e, 32 columns each): z chunks let a grid narrow in x
+// and y (a kmax unit cell) spread over every SM.  The default is 16 planes
+// of 8 rows; Solver::autotune times the candidates on a run's own steps.
+constexpr int UPD_ZCH = 16, UPD_TY = 8;
 
 // the complex instantiation at 3 CTAs per SM (80 registers, no spills): a
 // single unit cell's H takes 35.5 instead of 31.4 us, but concurrent runs
@@ -63,7 +63,7 @@ template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
-    const int py = blockIdx.y * 8 + threadIdx.y;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
     // H is updated on reference indices 1..N-1 of every axis (all positions
     // of a periodic axis)
     const int hx = P.per[0] ? P.SX - 1 : P.SX - 2;
@@ -89,8 +89,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
 
     // this CTA's z chunk (planes are independent: every plane reloads its
     // neighbours)
-    const int pz_end = min(hz, ((int)blockIdx.z + 1) * UPD_ZCH - 1);
-    for (int pz = blockIdx.z * UPD_ZCH; pz <= pz_end; pz++) {
+    const int pz_end = min(hz, ((int)blockIdx.z + 1) * P.zch_h - 1);
+    for (int pz = blockIdx.z * P.zch_h; pz <= pz_end; pz++) {
         bool wz;
         const int pzn = wrap_up(P, 2, pz, P.SZ, &wz);
         const int k = pz + 1;
@@ -343,7 +343,7 @@ template <typename T, bool DRUDE>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ? 2 : 3)) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
-    const int py = blockIdx.y * 8 + threadIdx.y;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
     __shared__ CoefTabs Tb;
     load_coef_tabs(P, Tb);
     if (px >= P.SX || py >= P.SY) return;
@@ -374,8 +374,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
     const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
     const bool x_unavg = !P.per[0] && i == 1, y_unavg = !P.per[1] && j == 1;
 
-    const int pz_end = min(P.SZ, ((int)blockIdx.z + 1) * UPD_ZCH);
-    for (int pz = blockIdx.z * UPD_ZCH; pz < pz_end; pz++) {
+    const int pz_end = min(P.SZ, ((int)blockIdx.z + 1) * P.zch_e);
+    for (int pz = blockIdx.z * P.zch_e; pz < pz_end; pz++) {
         const bool ex_u = ex_xy && upd(2, pz, false), ey_u = ey_xy && upd(2, pz, false), ez_u = ez_xy && upd(2, pz, true);
         if (!ex_u && !ey_u && !ez_u) continue;
         bool wzd;
@@ -541,14 +541,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
 }
 
 // ---------------------------------------------------------------------------
-int launch_update_h(const AemParams& P, int counter, cudaStream_t s) {
-    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8, (P.SZ + UPD_ZCH - 1) / UPD_ZCH);
+// a launch shape the caller did not set takes the default
+static void upd_shape(int& zch, int& ty) {
+    if (zch < 1) zch = UPD_ZCH;
+    if (ty < 1 || ty > 8) ty = UPD_TY;
+}
+
+int launch_update_h(const AemParams& Pin, int counter, cudaStream_t s) {
+    AemParams P = Pin;
+    upd_shape(P.zch_h, P.ty_h);
+    dim3 blk(32, P.ty_h), grd((P.SX + 31) / 32, (P.SY + P.ty_h - 1) / P.ty_h, (P.SZ + P.zch_h - 1) / P.zch_h);
     if (P.kmax) k_update_h<cf><<<grd, blk, 0, s>>>(P, counter);
     else k_update_h<float><<<grd, blk, 0, s>>>(P, counter);
     return 1;
 }
-int launch_update_e(const AemParams& P, int counter, cudaStream_t s) {
-    dim3 blk(32, 8), grd((P.SX + 31) / 32, (P.SY + 7) / 8, (P.SZ + UPD_ZCH - 1) / UPD_ZCH);
+int launch_update_e(const AemParams& Pin, int counter, cudaStream_t s) {
+    AemParams P = Pin;
+    upd_shape(P.zch_e, P.ty_e);
+    dim3 blk(32, P.ty_e), grd((P.SX + 31) / 32, (P.SY + P.ty_e - 1) / P.ty_e, (P.SZ + P.zch_e - 1) / P.zch_e);
     if (P.kmax) {
         if (P.has_drude) k_update_e<cf, true><<<grd, blk, 0, s>>>(P, counter);
         else k_update_e<cf, false><<<grd, blk, 0, s>>>(P, counter);

@@ -461,6 +461,7 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
         if ((size_t)f.gcount() != m.feeds[q].size() * sizeof(float)) throw DeckError("gridded feed file '" + path + "' is too short");
     }
     (void)any_grid;
+    if (d.ext_coef64) coef_tables_fp64(m);
 }
 
 }  // namespace aem

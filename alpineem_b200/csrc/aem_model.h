@@ -100,6 +100,12 @@ struct HostModel {
 // float32 material ids in the file's layout (x fastest).
 void build_model(HostModel& m, const std::string& workdir, const float* bulk = nullptr, size_t bulk_n = 0);
 
+// Extension `coef_precision 64`: recompute the material (Ga, Gb, Drude Ja,
+// Jb), CPML (b, c) and den tables on the current CUDA device in FP64, each
+// rounded to FP32 once (aem_coef.cu).  Throws std::runtime_error on a CUDA
+// failure.
+void coef_tables_fp64(HostModel& m);
+
 // Edge coefficients as the reference computes them from the averaged cell
 // properties (used by the host for sheet overrides and by tests).
 void edge_material(const HostModel& m, int comp, int i, int j, int k, float* eps, float* sig,

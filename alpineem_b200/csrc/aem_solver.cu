@@ -221,6 +221,8 @@ void Solver::setup_params() {
     const float mu0 = 1.25663706E-6f, ep0 = 8.85418782E-12f, c0 = 299792458.0f, pi = 3.14159265358979323846f;
     P.DB = d.del_t / mu0;
     P.dt = d.del_t;
+    P.zch_h = P.zch_e = 16;  // two-kernel launch shape until autotune picks one
+    P.ty_h = P.ty_e = 8;
     for (int c = 0; c < 3; c++) {
         P.E[c] = alloc((size_t)m_.cells * es_);
         P.H[c] = alloc((size_t)m_.cells * es_);
@@ -928,7 +930,53 @@ void Solver::watchdog_check() {
     if (bad) throw Diverged("the fields diverged: a non-finite value at step " + std::to_string(done_));
 }
 
+int Solver::autotune_pending(int budget) {
+    if (tuned_ || m_.d.ext_autotune <= 0 || budget <= 0) return 0;
+    const int d0 = done_;
+    autotune(m_.d.ext_autotune, nullptr, budget);
+    return done_ - d0;
+}
+
+void Solver::autotune(int per, int out[4], int budget) {
+    struct Shape {
+        int zch, ty;
+    };
+    // z planes per CTA, rows per CTA (32 columns each)
+    static const Shape cand[] = {{16, 8}, {8, 8}, {32, 8}, {4, 8}, {64, 8}, {16, 4}, {8, 4}, {32, 4}};
+    const int ncand = (int)(sizeof cand / sizeof cand[0]);
+    tuned_ = true;  // first: the tuning steps below go through run()
+    if (!fused_ && per > 0) {
+        const bool prof = prof_on_;
+        double best_h = 1e300, best_e = 1e300;
+        Shape bh = {P_.zch_h, P_.ty_h}, be = {P_.zch_e, P_.ty_e};
+        const int d0 = done_;
+        for (int c = 0; c < ncand && done_ + per <= m_.d.steps && done_ - d0 + per <= budget; c++) {
+            P_.zch_h = P_.zch_e = cand[c].zch;
+            P_.ty_h = P_.ty_e = cand[c].ty;
+            set_profiling(true);
+            run(per);
+            double ms[AEM_NPHASE];
+            long long nl[AEM_NPHASE];
+            read_profile(ms, nl);
+            // per launch (the split CPML order launches each kernel twice a step)
+            const double th = nl[AEM_PHASE_UPDATE_H] ? ms[AEM_PHASE_UPDATE_H] / nl[AEM_PHASE_UPDATE_H] : 1e300;
+            const double te = nl[AEM_PHASE_UPDATE_E] ? ms[AEM_PHASE_UPDATE_E] / nl[AEM_PHASE_UPDATE_E] : 1e300;
+            if (th < best_h) { best_h = th; bh = cand[c]; }
+            if (te < best_e) { best_e = te; be = cand[c]; }
+        }
+        P_.zch_h = bh.zch; P_.ty_h = bh.ty;
+        P_.zch_e = be.zch; P_.ty_e = be.ty;
+        set_profiling(prof);
+        release_graph();  // a captured graph holds the old shape
+    }
+    if (out) {
+        out[0] = P_.zch_h; out[1] = P_.ty_h;
+        out[2] = P_.zch_e; out[3] = P_.ty_e;
+    }
+}
+
 void Solver::run(int n) {
+    n -= autotune_pending(n);  // extension autotune: the tuning steps count towards n
     const int K = m_.d.ext_watchdog;
     for (int q = 0; q < n && done_ < m_.d.steps; q++) {
         done_++;
@@ -1112,6 +1160,7 @@ void Solver::run_batch(Solver* const* s, int count, int n, int g) {
     for (int i = 0; i < count; i++) {
         Solver& v = *s[i];
         left[i] = std::max(0, std::min(n, v.m_.d.steps - v.done_));
+        left[i] -= v.autotune_pending(left[i]);
         // eager steps until a chunk can start (at most one far-field batch)
         while (left[i] > 0 && !v.graph_ready(g) && (v.done_ == 0 || left[i] < g || v.FF_.tb > 1 && v.ff_n0_ != v.done_ + 1)) {
             v.run(1);

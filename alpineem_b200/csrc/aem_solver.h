@@ -40,6 +40,15 @@ class Solver {
     // run eagerly.  Graph chunks need g even on the fused path (the field
     // buffers swap each step) and g a multiple of the far-field batch.
     void run_graph(int n, int g);
+    // Launch shape of the two-kernel update, chosen by timing candidate
+    // shapes (z planes and rows per CTA) on the run's own next steps, up to
+    // `per` steps each; the fields do not depend on the shape.  Returns
+    // (z planes H, rows H, z planes E, rows E).  The fused path has nothing
+    // to tune.  The extension `autotune N` runs this at the first step.
+    void autotune(int per, int out[4], int budget = 1 << 30);
+    // the extension's tuning if it has not run yet, within `budget` steps;
+    // returns the steps it ran
+    int autotune_pending(int budget);
     // whole-run snapshot (device buffers of the setup, step counters) to a
     // file, and its restore into a handle made from the same deck
     void checkpoint_save(const std::string& path);
@@ -141,6 +150,7 @@ class Solver {
     int es_ = 4;  // bytes per field value
     int done_ = 0;
     bool fused_ = false;  // one fused H+E kernel per step (k_yee)
+    bool tuned_ = false;  // the two-kernel launch shape has been tuned (or need not be)
     bool split_ = false;  // bulk / port / CPML passes (a port inside a CPML slab)
     AemParams split_params_[2];
     int ff_n0_ = 1;  // first step held in the far-field difference buffer

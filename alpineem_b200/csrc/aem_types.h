@@ -129,6 +129,10 @@ struct AemParams {
     void* psi_h2[3][3][2];
     // device counter of fused-step CTAs that gave up a bounded wait (0 = ok)
     int* err;
+    // launch shape of the two-kernel update (k_update_h / k_update_e): z
+    // planes per CTA and rows (y) per CTA of 32 columns; the autotuner picks
+    // them per run and per kernel (the fields do not depend on them)
+    int zch_h, ty_h, zch_e, ty_e;
     // graph replay: the step number (1-based) lives in device memory and the
     // kernels read it instead of their `counter` argument (null: eager steps)
     const int* dstep;

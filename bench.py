@@ -243,8 +243,8 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
     another with plain launches, against the same instances advanced
     together by aem_run_batch (one stream per instance, one CUDA graph of g
     steps per instance).  Ranks take every world-th instance.  Setup, a
-    4-step warm-up of each run and the graph capture (one untimed chunk) are
-    outside both timings."""
+    warm-up of each run (4 steps and the launch-shape autotuning, 16 steps)
+    and the graph capture (one untimed chunk) are outside both timings."""
     import numpy as np
 
     import alpineem_b200 as ab
@@ -252,8 +252,11 @@ def batched_kmax(rank, world, steps, g, barrier, max_over_ranks):
     from alpineem_b200 import workloads
     from alpineem_b200.deck import deck_text
 
-    warm = 4
-    ext = workloads.KMAX_BATCH_EXT
+    # every instance tunes the launch shape of its update kernels during its
+    # warm-up (8 candidate shapes x 2 steps, extension `autotune 2`)
+    tune = 2
+    warm = 4 + 8 * tune
+    ext = workloads.KMAX_BATCH_EXT + "autotune %d\n" % tune
     kinds = ("reflected", "transmitted", "reflected_tm", "transmitted_tm")
     decks = shard(workloads.kmax_batch(steps=warm + 2 * g + steps), rank, world)
     tmp = tempfile.mkdtemp(prefix="aem_batch_")
@@ -389,7 +392,8 @@ def config_runs(max_over_ranks, world):
     out = {}
     for name, (deck, ext, _) in (("pec_sphere", workloads.pec_sphere()), ("layered_slab", workloads.layered_slab())):
         tmp = tempfile.mkdtemp(prefix="aem_cfg_")
-        sim = ab.Simulation(deck_text=deck_text(deck), ext_text=ext, outdir=tmp)
+        # the first 16 steps tune the update kernels' launch shape (inside the timing)
+        sim = ab.Simulation(deck_text=deck_text(deck), ext_text=ext + "autotune 2\n", outdir=tmp)
         cells, bytes_step = sim.workload
         steps = sim.steps[1]
         sim.synchronize()
@@ -400,6 +404,7 @@ def config_runs(max_over_ranks, world):
         wall = max_over_ranks(time.perf_counter() - t0)
         prof = sim.profile_read()
         sim.profile(False)
+        shape = sim.autotune(0)  # the shapes the run tuned (no further steps)
         sim.close()
         dev_ms = max_over_ranks(sum(v[0] for v in prof.values()))
         t_upd = (prof["update_h"][0] + prof["update_e"][0] + prof["yee"][0]) / steps / 1e3
@@ -408,7 +413,8 @@ def config_runs(max_over_ranks, world):
                      "wall_mcell_updates_per_s": round(world * cells * steps / wall / 1e6, 1),
                      "phases_ms_per_step": {k: round(v[0] / steps, 5) for k, v in prof.items() if v[1]},
                      "update_roofline_frac": round(bytes_step / t_upd / 1e9 / peak, 4),
-                     "update_path": "fused k_yee4" if prof["yee"][1] else "k_update_h + k_update_e"}
+                     "update_path": "fused k_yee4" if prof["yee"][1] else "k_update_h + k_update_e",
+                     "launch_shape": {k: {"z_planes": v[0], "rows": v[1]} for k, v in shape.items()}}
     return out
 
 

@@ -67,6 +67,11 @@ int aem_create_from_file(const char* inputs_path, int mode, const char* outdir, 
  *                    written to <name>_probes.dat (repeatable, at most 64)
  *   dft_freqs f0 f1 n   on-the-fly spectra (see aem_read_spectrum)
  *   watchdog K       check the fields for non-finite values every K steps
+ *   autotune N       tune the general update's launch shape at the first
+ *                    step, N steps per candidate (see aem_autotune)
+ *   coef_precision 64   material (Ga, Gb, Drude Ja, Jb) and CPML (b, c,
+ *                    kappa, den) tables evaluated on the GPU in FP64 and
+ *                    rounded once (reference: FP32, :2832-2918, :3404-3666)
  * `bulk` replaces the bulk geometry file the deck names (:2051-2055):
  * bulk_count float32 material ids, x fastest, (nx, ny, nz) cells; NULL/0
  * when the deck has none.  Side files (gridded feeds) and outputs resolve
@@ -92,6 +97,18 @@ int aem_run(aem_handle* h, int nsteps);
  * multiple of its 32-step batch.  No reference counterpart: the reference
  * launches every loop body from the host (fdtd_solver.f90:4440-8299). */
 int aem_run_graph(aem_handle* h, int nsteps, int steps_per_graph);
+
+/* Launch-shape autotuner of the general (two-kernel) H/E update: each of
+ * 8 candidate shapes (z planes per CTA 4..64, rows per CTA 4 or 8) runs
+ * the next `steps_per_candidate` steps of the run itself, timed with CUDA
+ * events; the fastest shape of each kernel is kept.  Every cell's
+ * arithmetic is the same under every shape, so the fields are those of an
+ * untuned run.  shape (may be NULL) receives z planes H, rows H, z planes
+ * E, rows E.  The fused path has no shape to tune (shape gets the unused
+ * defaults).  The sidecar extension `autotune N` does this at the first
+ * step.  No reference counterpart: the reference's OpenACC regions take the
+ * compiler's launch shapes (fdtd_solver.f90:4443 and the like). */
+int aem_autotune(aem_handle* h, int steps_per_candidate, int shape[4]);
 
 /* Advance `count` independent runs (distinct handles on the same device,
  * each on its own stream) by `nsteps` each, replaying their graphs

@@ -70,3 +70,42 @@ def test_fp32_error_against_fp64(name, tmp_path, oracle_bin, gpu_lib):
             f.write(json.dumps({"deck": name, "probe_rel_l2": probe, "far_field_rel_l2": ff}) + "\n")
     assert probe <= TOL_PROBE, (name, probe)
     assert ff <= TOL_FF, (name, ff)
+
+
+@pytest.mark.parametrize("name", ["tfsf_sphere", "drude_pbc", "kmax_te", "ellipsoids_small"])
+def test_fp64_coefficient_tables(name, tmp_path, oracle_bin, gpu_lib):
+    """Extension `coef_precision 64`: the material (Ga, Gb, Drude Ja, Jb) and
+    CPML (b, c, kappa, den) tables are evaluated on the GPU in FP64 and
+    rounded once.  The run then differs from the reference-arithmetic run
+    (the tables changed) and its probe series stay within 1e-4 of the FP64
+    oracle."""
+    import alpineem_b200 as ab
+    od, gd, rd = tmp_path / "f64", tmp_path / "gpu64", tmp_path / "gpu32"
+    for p in (od, gd, rd):
+        p.mkdir()
+    _, kmax = decks.write_deck(name, str(od))
+    decks.write_deck(name, str(gd))
+    decks.write_deck(name, str(rd))
+    ext = gd / "inputs.txt.b200"
+    ext.write_text((ext.read_text() if ext.exists() else "") + "coef_precision 64\n")
+    _run_oracle(oracle_bin["fdtd_oracle_kmax_f64" if kmax else "fdtd_oracle_f64"], str(od))
+    for d in (gd, rd):
+        with ab.Simulation(str(d / "inputs.txt"), kmax=kmax, outdir=str(d)) as sim:
+            sim.run_all()
+    fname = decks.DECKS[name].get("name", "data.dat")
+    ob, _ = dat_blocks(str(od / fname))
+    gb, _ = dat_blocks(str(gd / fname))
+    rb, _ = dat_blocks(str(rd / fname))
+    peak = max(np.linalg.norm(b) for _, b in ob)
+    probe, changed = 0.0, False
+    for (ta, a), (_, b), (_, c) in zip(ob, gb, rb):
+        changed = changed or not np.array_equal(b, c)
+        if ta.startswith("far field rE") or ta.startswith("far field phase correction"):
+            continue
+        probe = max(probe, rel_l2(a, b, floor=1e-3 * peak))
+    rep = os.environ.get("AEM_PRECISION_REPORT")
+    if rep:
+        with open(rep, "a") as f:
+            f.write(json.dumps({"deck": name + "_coef64", "probe_rel_l2": probe}) + "\n")
+    assert changed, name
+    assert probe <= TOL_PROBE, (name, probe)
