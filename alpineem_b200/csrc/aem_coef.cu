@@ -33,6 +33,7 @@ struct CoefIn {
     double dt;
     int npml[3][2];
     int N[3];
+    long long den_off[3];  // first den_h value of axis a (den_e follows N[a] + 1 later)
     double dl[3], sig_max[3], alpha_max, kappa_max;
 };
 
@@ -122,8 +123,8 @@ __global__ void k_coef_fp64(const AemMaterial* mats, CoefIn in, AemUniformCoef* 
             if (i <= n1) ve = 1.0 / (kap(0, i, true) * in.dl[a]);
             else if (i >= Na + 1 - n2) ve = 1.0 / (kap(1, Na + 1 - i, true) * in.dl[a]);
             else ve = 1.0 / in.dl[a];
-            den[((size_t)a * 2 + 0) * (Na + 1) + i - 1] = (float)vh;
-            den[((size_t)a * 2 + 1) * (Na + 1) + i - 1] = (float)ve;
+            den[in.den_off[a] + i - 1] = (float)vh;
+            den[in.den_off[a] + (Na + 1) + i - 1] = (float)ve;
             return;
         }
         u -= Na - 1;
@@ -158,7 +159,10 @@ void coef_tables_fp64(HostModel& m) {
     in.kappa_max = (double)d.kappa_max;
     const size_t cp_n = (size_t)3 * 2 * 6 * CP_STRIDE;
     size_t den_n = 0;
-    for (int a = 0; a < 3; a++) den_n += (size_t)2 * (N[a] + 1);
+    for (int a = 0; a < 3; a++) {
+        in.den_off[a] = (long long)den_n;
+        den_n += (size_t)2 * (N[a] + 1);
+    }
     AemMaterial* dm = nullptr;
     AemUniformCoef* du = nullptr;
     float *dc = nullptr, *dd = nullptr;

@@ -563,8 +563,8 @@ void Solver::setup_farfield() {
             // per (j, face): tiles sorted by (kb, tile), for the ordered reduction
             std::vector<int> srt((size_t)F.nvc * 6 * F.maxt, 0), srtkb((size_t)F.nvc * 6 * F.maxt, INT_MAX);
             std::vector<int> kbmin((size_t)F.nvc, INT_MAX), kbmax((size_t)F.nvc, INT_MIN);
-            std::vector<int> idx;
-            for (int j = 0; j < F.nvc; j++)
+            par_for(F.nvc, [&](int j) {  // each angle writes its own lists
+                std::vector<int> idx;
                 for (int f = 0; f < 6; f++) {
                     const int t0 = (int)F.tile0[f], nt = (int)(F.tile0[f + 1] - F.tile0[f]);
                     idx.resize(nt);
@@ -583,6 +583,7 @@ void Solver::setup_farfield() {
                         kbmax[j] = std::max(kbmax[j], srtkb[o + nt - 1]);
                     }
                 }
+            });
             F.srt = (const int*)upload(srt);
             F.srtkb = (const int*)upload(srtkb);
             // reduction CTAs: the canonical angles, with the j of each pass
