@@ -27,7 +27,7 @@ HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "alpineem_b200.h")
 STANDARD, KMAX = 0, 1
 SERIES = {"incident": 0, "reflected": 1, "transmitted": 2, "reflected_tm": 3, "transmitted_tm": 4,
           "port_voltage": 5, "e_theta": 6, "e_phi": 7}
-FIELDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
+FIELDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5, "material": 6}
 # per-step samples that aem_read_probe returns; "point" is the extension
 # `probe i j k` (index 3 p + c: probe p, component c = Ex, Ey, Ez)
 PROBE_KINDS = {"reflected": 1, "transmitted": 2, "reflected_tm": 3, "transmitted_tm": 4, "port_voltage": 5,
@@ -257,7 +257,8 @@ class Simulation:
         return (re[:m] + 1j * im[:m]) if self.kmax else re[:m]
 
     def field(self, comp):
-        """Final field component in the reference's layout, shape (nz, ny, nx) of F-order (x fastest)."""
+        """Final field component in the reference's layout, shape (nz, ny, nx) of F-order (x fastest);
+        "material" gives the cells' material indices (0 = background, r = r-th volume material)."""
         c = FIELDS[comp] if isinstance(comp, str) else int(comp)
         dims = (ctypes.c_int * 3)()
         self._check(self._lib.aem_get_field(self._h, c, dims, None, None))
@@ -266,6 +267,8 @@ class Simulation:
         self._check(self._lib.aem_get_field(self._h, c, dims, _dptr(re), _dptr(im)))
         shape = (dims[2], dims[1], dims[0])
         out = re.reshape(shape)
+        if c == 6:
+            return out.astype(np.uint8)
         return out + 1j * im.reshape(shape) if self.kmax else out
 
     def probe(self, kind, index=0, first=1, n=None):

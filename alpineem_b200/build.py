@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-ftz=true", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + ARCH
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-pthread", "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU = ["aem_kernels.cu", "aem_yee.cu", "aem_yee4.cu", "aem_aux.cu", "aem_ffbin.cu", "aem_coef.cu", "aem_dft.cu", "aem_dft_static.cu", "aem_solver.cu", "aem_finalize.cu", "aem_design.cu"]
+CU = ["aem_kernels.cu", "aem_yee.cu", "aem_yee4.cu", "aem_aux.cu", "aem_ffbin.cu", "aem_coef.cu", "aem_raster.cu", "aem_dft.cu", "aem_dft_static.cu", "aem_solver.cu", "aem_finalize.cu", "aem_design.cu"]
 CPP = ["aem_deck.cpp", "aem_model.cpp", "aem_api.cpp"]
 HEADERS = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".h", ".cuh"))] + [
     os.path.join(ROOT, "include", "alpineem_b200.h")]

@@ -211,7 +211,7 @@ int aem_get_series(aem_handle* h, int kind, int index, double* re, double* im, i
 }
 
 int aem_get_field(aem_handle* h, int comp, int dims[3], double* re, double* im) {
-    if (!h || !dims || comp < 0 || comp > 5) return fail(h, AEM_ERR_ARG, "bad argument");
+    if (!h || !dims || comp < 0 || comp > 6) return fail(h, AEM_ERR_ARG, "bad argument");
     return guarded(h, [&]() {
         std::vector<double> r, i;
         h->s->get_field(comp, r, i, dims);

@@ -381,10 +381,26 @@ void Solver::finalize_and_write() {
     }
 }
 
-// final field component in the reference's own array layout
+// final field component in the reference's own array layout; comp 6 gives
+// the per-cell material indices the run uses (0 = vacuum, r = r-th volume
+// material of the deck)
 void Solver::get_field(int comp, std::vector<double>& re, std::vector<double>& im, int dims[3]) {
     const Deck& d = m_.d;
     const int X = d.X, Y = d.Y, Z = d.Z;
+    if (comp == 6) {  // the cells' material indices, cells 1..N-1 (not a periodic axis' duplicate)
+        for (int a = 0; a < 3; a++) dims[a] = (a == 0 ? X : a == 1 ? Y : Z) - 1 - d.pbc[a];
+        std::vector<uint8_t> ids((size_t)m_.cells);
+        AEM_CUDA(cudaMemcpyAsync(ids.data(), P_.cell, ids.size(), cudaMemcpyDeviceToHost, stream_));
+        AEM_CUDA(cudaStreamSynchronize(stream_));
+        d2h_bytes_ += ids.size();
+        re.assign((size_t)dims[0] * dims[1] * dims[2], 0.0);
+        im.assign(re.size(), 0.0);
+        for (int k = 1; k <= dims[2]; k++)
+            for (int j = 1; j <= dims[1]; j++)
+                for (int i = 1; i <= dims[0]; i++)
+                    re[((size_t)(k - 1) * dims[1] + (j - 1)) * dims[0] + (i - 1)] = ids[m_.lin(i, j, k)];
+        return;
+    }
     static const int ext[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {0, -1, -1}, {-1, 0, -1}, {-1, -1, 0}};
     dims[0] = X + ext[comp][0]; dims[1] = Y + ext[comp][1]; dims[2] = Z + ext[comp][2];
     std::vector<cplx> all = fetch(comp < 3 ? P_.E[comp] : P_.H[comp - 3], (size_t)m_.cells, d.kmax, stream_, d2h_bytes_);

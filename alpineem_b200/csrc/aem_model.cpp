@@ -16,6 +16,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -163,9 +164,19 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
         return true;
     };
 
+    // the host reads the ids for sheet overrides, Drude boxes and the
+    // geometry output; without those the device rasterises them
+    // (AEM_HOST_RASTER=1 keeps the host builder, for comparison)
+    const char* host_env = std::getenv("AEM_HOST_RASTER");
+    m.raster_device = d.sheets.empty() && !is_plasma && !d.ext_geometry_bin && !(host_env && host_env[0] == '1');
+    m.raster_bulk = nullptr;
+    m.raster_file.clear();
+    m.raster_map.clear();
     m.cell_id.clear();
-    m.cell_id.resize((size_t)m.cells);  // uninitialised: zeroed plane by plane in parallel
-    par_for(m.S[2], [&](int z) { std::memset(m.cell_id.data() + (size_t)z * m.plane, 0, (size_t)m.plane); });
+    if (!m.raster_device) {
+        m.cell_id.resize((size_t)m.cells);  // uninitialised: zeroed plane by plane in parallel
+        par_for(m.S[2], [&](int z) { std::memset(m.cell_id.data() + (size_t)z * m.plane, 0, (size_t)m.plane); });
+    }
     if (!d.bulk_file.empty()) {  // ref :2051-2095
         const size_t nbulk = (size_t)gx * gy * gz;
         std::vector<float> file_data;
@@ -177,16 +188,20 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
             std::string path = resolve(workdir, d.bulk_file);
             std::ifstream f(path, std::ios::binary);
             if (!f) throw DeckError("cannot open bulk geometry file '" + path + "'");
-            file_data.resize(nbulk);
-            f.read((char*)file_data.data(), (std::streamsize)(nbulk * sizeof(float)));
+            std::vector<float>& fd = m.raster_device ? m.raster_file : file_data;
+            fd.resize(nbulk);
+            f.read((char*)fd.data(), (std::streamsize)(nbulk * sizeof(float)));
             if ((size_t)f.gcount() != nbulk * sizeof(float)) throw DeckError("bulk geometry file '" + path + "' is too short");
-            bg = file_data.data();
+            bg = fd.data();
         }
         int mx = 0;
         for (auto& vm : d.mats) mx = std::max(mx, (int)vm.id);
         std::vector<int> tmp((size_t)mx + 1, 0);
         for (size_t r = 0; r < d.mats.size(); r++) tmp[(int)d.mats[r].id] = (int)r + 1;
-        par_for(gz, [&](int kk) {  // planes write disjoint cells
+        if (m.raster_device) {
+            m.raster_bulk = bg;
+            m.raster_map = std::move(tmp);
+        } else par_for(gz, [&](int kk) {  // planes write disjoint cells
             const int k = kk + 1;
             for (int j = 1; j <= gy; j++)
                 for (int i = 1; i <= gx; i++) {
@@ -200,6 +215,7 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk, si
     }
     int mid = 0;
     for (auto& o : d.objects) {  // ref :2101-2288
+        if (m.raster_device) break;  // objects are drawn by the device, in the same order
         mid = find_mat((float)o.mat, mid);
         auto put = [&](int i, int j, int k) {
             if (cell_ok(i, j, k)) m.cell_id[m.lin(i, j, k)] = (uint8_t)mid;

@@ -78,6 +78,16 @@ struct HostModel {
     std::vector<std::vector<float>> feeds;        // per port: gridded feed (4, n1+1, n2+1), F-order
     int feed_m1 = 0, feed_m2 = 0;                 // reference array extents (max n1+1, max n2+1)
     std::vector<float> geometry;                  // (4, gx, gy, gz) F-order float32 for _geometry.bin
+    // When no host step reads the ids (no sheets, no Drude poles, no
+    // _geometry.bin) cell_id stays empty and the ids are rasterised on the
+    // device (rasterise_device): raster_bulk points at the bulk ids in the
+    // file's layout (the caller's buffer or raster_file) and raster_map
+    // maps a file id to its material index.  Valid until the solver's setup
+    // has uploaded them.
+    bool raster_device = false;
+    const float* raster_bulk = nullptr;
+    std::vector<float> raster_file;
+    std::vector<int> raster_map;
 
     // storage position of reference index `idx` on axis a (wraps when periodic)
     int pos(int a, int idx) const {
@@ -105,6 +115,13 @@ void build_model(HostModel& m, const std::string& workdir, const float* bulk = n
 // rounded to FP32 once (aem_coef.cu).  Throws std::runtime_error on a CUDA
 // failure.
 void coef_tables_fp64(HostModel& m);
+
+// The per-cell material ids of a model built with raster_device set,
+// written into the zeroed device array `cell` ([SZ][SY][PX]) on stream `s`
+// (aem_raster.cu): the same ids the host builder writes.  Adds the bytes
+// copied to the device to `h2d`; returns after the stream has finished.
+// Throws std::runtime_error on a CUDA failure.
+void rasterise_device(const HostModel& m, uint8_t* cell, struct CUstream_st* s, size_t& h2d);
 
 // Edge coefficients as the reference computes them from the averaged cell
 // properties (used by the host for sheet overrides and by tests).

@@ -227,7 +227,15 @@ void Solver::setup_params() {
         P.E[c] = alloc((size_t)m_.cells * es_);
         P.H[c] = alloc((size_t)m_.cells * es_);
     }
-    P.cell = (const uint8_t*)upload(m_.cell_id);
+    if (m_.raster_device) {
+        uint8_t* ids = (uint8_t*)alloc((size_t)m_.cells);  // zeroed on stream_
+        rasterise_device(m_, ids, stream_, h2d_bytes_);
+        P.cell = ids;
+        m_.raster_bulk = nullptr;  // the caller's buffer is not kept
+        std::vector<float>().swap(m_.raster_file);
+    } else {
+        P.cell = (const uint8_t*)upload(m_.cell_id);
+    }
     for (int a = 0; a < 3; a++) {
         P.npml[a][0] = d.npml[a][0];
         P.npml[a][1] = d.npml[a][1];

@@ -260,9 +260,12 @@ int aem_get_series(aem_handle* h, int kind, int index, double* re, double* im, i
 
 /* Final field component in the reference's array layout (first index
  * fastest): comp 0..5 = Ex, Ey, Ez, Hx, Hy, Hz with the extents of
- * fdtd_solver.f90:3908-3913.  `dims` receives the extents; re/im must hold
- * dims[0]*dims[1]*dims[2] values (pass NULL first to query dims).  im may be
- * NULL. */
+ * fdtd_solver.f90:3908-3913.  comp 6 = each cell's material index as the
+ * run uses it (0 = background, r = the deck's r-th volume material) over
+ * cells 1..N-1 of each axis, a periodic axis' duplicated layer left out
+ * (the extents of <name>_geometry.bin).  `dims` receives the extents;
+ * re/im must hold dims[0]*dims[1]*dims[2] values (pass NULL first to query
+ * dims).  im may be NULL. */
 int aem_get_field(aem_handle* h, int comp, int dims[3], double* re, double* im);
 
 /* Reference grid sizes X, Y, Z (cells per axis + 1 + periodic layer,

@@ -167,6 +167,42 @@ DECKS["kmax_ff"] = dict(kmax=True, n=(36, 10, 10), dl=("0.25E-3", "0.25E-3", "0.
                         mats=[("simple", 5, (4, 4, 4), (0, 0, 0))], objects=[("block", 5, (14, 1, 1), (8, 10, 10))])
 
 
+def _raster_bulk(shape, seed, ids):
+    """Bulk ids (gz, gy, gx) drawn from `ids` (fractional values truncate,
+    negative and unknown ones leave the background)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return rng.choice(np.array(ids, np.float32), size=shape)
+
+
+# --- decks of the device rasteriser (no sheets, Drude poles or geometry
+# output, so the ids are drawn on the GPU): a bulk file of random ids
+# (unknown, negative and fractional values among them) under objects of
+# every kind reaching the grid's faces and the periodic duplicate layer,
+# overlapping one another, one with a material id the deck does not define
+# (it keeps the previous object's material, ref :2101-2288).  Every object
+# stays inside the grid: the reference writes cells outside it out of its
+# arrays' bounds
+DECKS["raster_pbc_x"] = dict(
+    n=(40, 30, 34), steps=160, f="15E9", pulse=1, bc=(1, 1, 0, 0, 0, 0), excitation=("antenna", 1, 0, 1),
+    ff=[(90, 0), (50, 100)], ffc=(20, 15, 17), bulk="ids.bin",
+    mats=[("simple", 2, (2, 2, 2), (0.01, 0.01, 0.01)), ("simple", 3, (3, 2.5, 4), (0, 0, 0)),
+          ("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (1.5, 1.5, 1.5), (0.002, 0, 0))],
+    objects=[("block", 3, (33, 3, 5), (9, 6, 6)), ("sphere", 5, (6, 12, 20), 5), ("sphere", 9, (30, 22, 10), 3),
+             ("cylinder", 2, "x", (1, 8, 27), (41, 3)), ("cylinder", 3, "y", (28, 1, 6), (30, 2)),
+             ("block", 4, (20, 15, 12), (1, 1, 5)), ("block", 4, (20, 15, 18), (1, 1, 5))],
+    ports=[("basic", "z", 50, (20, 15, 17), (1, 1, 1))],
+    _ext="geometry_bin no\n", _bulk=_raster_bulk((34, 30, 40), 11, [0, 0, 0, 2, 3, 3.7, 5, 9, -1]))
+DECKS["raster_pbc_yz"] = dict(
+    n=(40, 12, 14), dl=("0.5E-3", "0.5E-3", "0.5E-3"), steps=300, f="8E9", bc=(0, 0, 1, 1, 1, 1),
+    excitation=("plane wave", 1, 0, 90, 0, 90), bulk="ids.bin",
+    mats=[("simple", 2, (2, 2, 2), (0.01, 0.01, 0.01)), ("simple", 3, (3, 2.5, 4), (0, 0, 0)),
+          ("simple", 5, (1.5, 1.5, 1.5), (0.002, 0, 0))],
+    objects=[("sphere", 3, (20, 5, 8), 4), ("cylinder", 5, "z", (26, 10, 1), (15, 3)),
+             ("block", 2, (30, 9, 10), (4, 5, 6)), ("cylinder", 3, "x", (6, 6, 7), (3, 0))],
+    _ext="geometry_bin no\n", _bulk=_raster_bulk((14, 12, 40), 12, [0, 0, 2, 3, 5, 5.5, 7, -3]))
+
+
 def write_deck(name, directory, fname="inputs.txt"):
     """Write deck `name` (and its sidecar / bulk geometry file, if any) into
     `directory`; returns (path, kmax)."""
