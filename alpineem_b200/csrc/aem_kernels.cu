@@ -56,9 +56,14 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
 // of 8 rows; Solver::autotune times the candidates on a run's own steps.
 constexpr int UPD_ZCH = 16, UPD_TY = 8;
 
-// the complex instantiation at 3 CTAs per SM (80 registers, no spills): a
-// single unit cell's H takes 35.5 instead of 31.4 us, but concurrent runs
-// of a batched constant-k sweep overlap better (18.2 vs 17.2 Gcell/s)
+// One thread per (x, y) column marching its z chunk.  The per-cell work
+// every position shares (bulk curl, CPML psi terms, periodic wraps) is
+// straight-line code with per-lane predicates, so lanes in a CPML slab or
+// at a wrap do not split a warp into two code paths; the rare corrections
+// (sheet planes, TF/SF faces, the constant-k source plane) sit behind one
+// flag per position, made of a column test done once and a plane test
+// done per plane.  E(k+1) stays in registers as the next plane's E(k).
+// The complex instantiation runs at 3 CTAs per SM (no spills).
 template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
@@ -77,6 +82,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
     bool wx, wy;
     const int pxn = wrap_up(P, 0, px, P.SX, &wx);
     const int pyn = wrap_up(P, 1, py, P.SY, &wy);
+    const long long plane = (long long)P.SY * P.PX;
+    const long long offx = pxn - px, offy = (long long)(pyn - py) * P.PX;  // +x / +y neighbours
     const int i = px + 1, j = py + 1;
     const float DB = P.DB;
     const float dhx = P.den_h[0][i - 1], dhy = P.den_h[1][j - 1];
@@ -86,23 +93,44 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
     const int qx_hi = (i >= P.X + 1 - P.npml[0][1]) ? P.X - i : 0;
     const int qy_lo = (j <= P.npml[1][0] - 1) ? j : 0;
     const int qy_hi = (j >= P.Y + 1 - P.npml[1][1]) ? P.Y - j : 0;
+    const bool col_cpml = qx_lo || qx_hi || qy_lo || qy_hi;
+    // rare corrections that this column can take: an x or y sheet plane
+    // through it, a TF/SF x or y face, the constant-k source plane
+    bool col_rare = false;
+    for (int s = 0; s < P.nsheet; s++)
+        col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
+    if (sizeof(T) == sizeof(float) && P.tfsf_on)
+        col_rare |= (!P.per[0] && (i == P.lo[0] - 1 || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] - 1 || j == P.hi[1]));
+    if (sizeof(T) != sizeof(float) && P.kmax_mode_TE)
+        col_rare |= (P.kmax_src_axis == 0 && i == P.k_pl_H) || (P.kmax_src_axis == 1 && j == P.k_pl_H);
 
-    // this CTA's z chunk (planes are independent: every plane reloads its
-    // neighbours)
+    // this CTA's z chunk
+    const int pz0 = blockIdx.z * P.zch_h;
     const int pz_end = min(hz, ((int)blockIdx.z + 1) * P.zch_h - 1);
-    for (int pz = blockIdx.z * P.zch_h; pz <= pz_end; pz++) {
+    long long c = lin(P, px, py, pz0);
+    T ex = zero<T>(), ey = zero<T>();
+    bool have = false;  // ex, ey of this plane were loaded as the previous plane's +z neighbours
+    for (int pz = pz0; pz <= pz_end; pz++, c += plane) {
         bool wz;
         const int pzn = wrap_up(P, 2, pz, P.SZ, &wz);
+        const long long offz = (long long)(pzn - pz) * plane;
         const int k = pz + 1;
-        const long long c = lin(P, px, py, pz);
         const float dhz = P.den_h[2][k - 1];
-        const T ex = ld<T>(Ex, c), ey = ld<T>(Ey, c), ez = ld<T>(Ez, c);
-        const T ex_jp = ld_up<T>(P, Ex, lin(P, px, pyn, pz), wy, 1);
-        const T ex_kp = ld_up<T>(P, Ex, lin(P, px, py, pzn), wz, 2);
-        const T ey_ip = ld_up<T>(P, Ey, lin(P, pxn, py, pz), wx, 0);
-        const T ey_kp = ld_up<T>(P, Ey, lin(P, px, py, pzn), wz, 2);
-        const T ez_ip = ld_up<T>(P, Ez, lin(P, pxn, py, pz), wx, 0);
-        const T ez_jp = ld_up<T>(P, Ez, lin(P, px, pyn, pz), wy, 1);
+        if (!have) {
+            ex = ld<T>(Ex, c);
+            ey = ld<T>(Ey, c);
+        }
+        const T ez = ld<T>(Ez, c);
+        const T ex_jp = ld_up<T>(P, Ex, c + offy, wy, 1);
+        const T ex_kp = ld_up<T>(P, Ex, c + offz, wz, 2);
+        const T ey_ip = ld_up<T>(P, Ey, c + offx, wx, 0);
+        const T ey_kp = ld_up<T>(P, Ey, c + offz, wz, 2);
+        const T ez_ip = ld_up<T>(P, Ez, c + offx, wx, 0);
+        const T ez_jp = ld_up<T>(P, Ez, c + offy, wy, 1);
+        bool rare = col_rare;
+        for (int s = 0; s < P.nsheet; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
+        if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] - 1 || k == P.hi[2]);
+        if (sizeof(T) != sizeof(float) && P.kmax_mode_TE) rare |= P.kmax_src_axis == 2 && k == P.k_pl_H;
 
         T hxv = ld<T>(Hx, c), hyv = ld<T>(Hy, c), hzv = ld<T>(Hz, c);
         if (P.cpml_split != 2) {
@@ -111,6 +139,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
         hyv = hyv + DB * ((ez_ip - ez) * dhx + (ex - ex_kp) * dhz);
         hzv = hzv + DB * ((ey - ey_ip) * dhx + (ex_jp - ex) * dhy);
 
+        if (rare) {
         // Smith-Maloney sheets, ref :4486-4554
         for (int s = 0; s < P.nsheet; s++) {
             const AemSheetPlane& S = P.sheet[s];
@@ -215,12 +244,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
                 }
             }
         }
+        }  // rare
 
         }  // cpml_split != 2
         // CPML on H, ref :5227-5375: Hx (y then z), Hy (x then z), Hz (x then y)
-        if (P.cpml_split != 1) {
-            const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0;
-            const int qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
+        const int qz_lo = (k <= P.npml[2][0] - 1) ? k : 0;
+        const int qz_hi = (k >= P.Z + 1 - P.npml[2][1]) ? P.Z - k : 0;
+        if (P.cpml_split != 1 && (col_cpml || qz_lo || qz_hi)) {
             if (qy_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][0], Tb.bh[1][0][qy_lo - 1], Tb.ch[1][0][qy_lo - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_lo, px, py, pz, P.npml[1][0]));
             if (qy_hi) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][1][1], Tb.bh[1][1][qy_hi - 1], Tb.ch[1][1][qy_hi - 1], ez - ez_jp, P.del[1], psi_idx(P, 1, qy_hi, px, py, pz, P.npml[1][1]));
             if (qz_lo) hxv = hxv + DB * cpml_term<T>(P, P.psi_h[0][2][0], Tb.bh[2][0][qz_lo - 1], Tb.ch[2][0][qz_lo - 1], ey_kp - ey, P.del[2], psi_idx(P, 2, qz_lo, px, py, pz, P.npml[2][0]));
@@ -237,6 +267,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
         st<T>(Hx, c, hxv);
         st<T>(Hy, c, hyv);
         st<T>(Hz, c, hzv);
+        // E(k+1) is the next plane's E(k) (not across a periodic wrap)
+        ex = ex_kp;
+        ey = ey_kp;
+        have = !wz;
     }
 }
 
@@ -337,10 +371,14 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
     return rk >= b[0] && rk <= b[1] && rj >= b[2] && rj <= b[3] && ri >= b[4] && ri <= b[5];
 }
 
-// DRUDE: the instantiation for decks with Drude poles; without the ADE
-// code the complex kernel fits 3 CTAs per SM (80 registers, no spills)
+// DRUDE: the instantiation for decks with Drude poles.  Same structure as
+// k_update_h: CPML, walls and wraps are per-lane work on the common path,
+// sheets, Drude boxes, TF/SF faces and the constant-k source plane sit
+// behind one flag per position, and H(k-1) and the ids of plane k-1 come
+// from the previous plane.  3 CTAs per SM (FP32, 80 registers) and 2
+// (complex) leave room for both paths' registers.
 template <typename T, bool DRUDE>
-__global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ? 2 : 3)) k_update_e(const __grid_constant__ AemParams P, int counter) {
+__global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : 2) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -373,14 +411,46 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
     const int qxl = (i >= 2 && i <= P.npml[0][0]) ? i : 0, qxh = (i >= P.X + 1 - P.npml[0][1] && i <= P.X - 1) ? P.X + 1 - i : 0;
     const int qyl = (j >= 2 && j <= P.npml[1][0]) ? j : 0, qyh = (j >= P.Y + 1 - P.npml[1][1] && j <= P.Y - 1) ? P.Y + 1 - j : 0;
     const bool x_unavg = !P.per[0] && i == 1, y_unavg = !P.per[1] && j == 1;
+    const long long plane = (long long)P.SY * P.PX;
+    const long long offx = pxd - px, offy = (long long)(pyd - py) * P.PX;  // -x / -y neighbours
+    const bool col_cpml = qxl || qxh || qyl || qyh;
+    // rare corrections that this column can take: an x or y sheet plane
+    // through it, a TF/SF x or y face, the constant-k source plane, a
+    // Drude box over it
+    bool col_rare = false;
+    for (int s = 0; s < P.nsheet; s++)
+        col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
+    if (sizeof(T) == sizeof(float) && P.tfsf_on)
+        col_rare |= (!P.per[0] && (i == P.lo[0] || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] || j == P.hi[1]));
+    if (sizeof(T) != sizeof(float) && P.kmax_mode_TM)
+        col_rare |= (P.kmax_src_axis == 0 && (i == P.k_pl_E || rix_t == P.k_pl_E)) ||
+                    (P.kmax_src_axis == 1 && (j == P.k_pl_E || riy_t == P.k_pl_E));
+    bool col_drude = false;
+    if (DRUDE && P.has_drude)
+        for (int cc = 0; cc < 3; cc++) {
+            const int* b = P.dbox[cc];
+            const int ri = cc == 0 ? i : rix_t, rj = cc == 1 ? j : riy_t;
+            col_drude |= rj >= b[2] && rj <= b[3] && ri >= b[4] && ri <= b[5];
+        }
 
+    const int pz0 = blockIdx.z * P.zch_e;
     const int pz_end = min(P.SZ, ((int)blockIdx.z + 1) * P.zch_e);
-    for (int pz = blockIdx.z * P.zch_e; pz < pz_end; pz++) {
+    long long c = lin(P, px, py, pz0);
+    // H(k-1) and the ids of plane k-1 from the previous plane
+    T hx_prev = zero<T>(), hy_prev = zero<T>();
+    int id0_prev = 0, idx_prev = 0, idy_prev = 0;
+    bool have = false;
+    for (int pz = pz0; pz < pz_end; pz++, c += plane) {
         const bool ex_u = ex_xy && upd(2, pz, false), ey_u = ey_xy && upd(2, pz, false), ez_u = ez_xy && upd(2, pz, true);
-        if (!ex_u && !ey_u && !ez_u) continue;
+        if (!ex_u && !ey_u && !ez_u) {
+            have = false;
+            continue;
+        }
         bool wzd;
         int pzd = wrap_dn(P, 2, pz, P.SZ, &wzd);
         if (pzd < 0) pzd = 0;
+        const long long offz = (long long)(pzd - pz) * plane;
+        const bool reuse = have && !wzd;
         const int k = pz + 1;
         const int riz_t = rep_idx(P, 2, pz, true);
         const float dez = P.den_e[2][k - 1];
@@ -390,20 +460,41 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
         // thread waits on one round of memory latency instead of one per
         // component.  A neighbour index of a component not updated here is
         // clamped to 0 above and its value is not used.
-        const long long c = lin(P, px, py, pz);
-        const long long cxm = lin(P, pxd, py, pz), cym = lin(P, px, pyd, pz), czm = lin(P, px, py, pzd);
         const T hx = ld<T>(Hx, c), hy = ld<T>(Hy, c), hz = ld<T>(Hz, c);
-        const T hz_jm = ld_dn<T>(P, Hz, cym, wyd, 1), hy_km = ld_dn<T>(P, Hy, czm, wzd, 2);
-        const T hz_im = ld_dn<T>(P, Hz, cxm, wxd, 0), hx_km = ld_dn<T>(P, Hx, czm, wzd, 2);
-        const T hy_im = ld_dn<T>(P, Hy, cxm, wxd, 0), hx_jm = ld_dn<T>(P, Hx, cym, wyd, 1);
+        const T hz_jm = ld_dn<T>(P, Hz, c + offy, wyd, 1);
+        const T hy_km = reuse ? hy_prev : ld_dn<T>(P, Hy, c + offz, wzd, 2);
+        const T hz_im = ld_dn<T>(P, Hz, c + offx, wxd, 0);
+        const T hx_km = reuse ? hx_prev : ld_dn<T>(P, Hx, c + offz, wzd, 2);
+        const T hy_im = ld_dn<T>(P, Hy, c + offx, wxd, 0), hx_jm = ld_dn<T>(P, Hx, c + offy, wyd, 1);
         const T eo0 = ld<T>(Ex, c), eo1 = ld<T>(Ey, c), eo2 = ld<T>(Ez, c);
         // the seven cells around this position's three edges, ref :2516-2527
         int id0 = 0, idx = 0, idy = 0, idz = 0, idxy = 0, idxz = 0, idyz = 0;
         if (!unavg) {
             const uint8_t* C = P.cell;
-            id0 = C[c]; idx = C[cxm]; idy = C[cym]; idz = C[czm];
-            idxy = C[lin(P, pxd, pyd, pz)]; idxz = C[lin(P, pxd, py, pzd)]; idyz = C[lin(P, px, pyd, pzd)];
+            id0 = C[c]; idx = C[c + offx]; idy = C[c + offy]; idxy = C[c + offx + offy];
+            if (reuse) {
+                idz = id0_prev; idxz = idx_prev; idyz = idy_prev;
+            } else {
+                idz = C[c + offz]; idxz = C[c + offx + offz]; idyz = C[c + offy + offz];
+            }
         }
+        hx_prev = hx;
+        hy_prev = hy;
+        id0_prev = id0;
+        idx_prev = idx;
+        idy_prev = idy;
+        have = !unavg;  // the ids of this plane were read
+        bool rare = col_rare;
+        for (int s = 0; s < P.nsheet; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
+        if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] || k == P.hi[2]);
+        if (sizeof(T) != sizeof(float) && P.kmax_mode_TM)
+            rare |= P.kmax_src_axis == 2 && (k == P.k_pl_E || riz_t == P.k_pl_E);
+        if (col_drude)
+            for (int cc = 0; cc < 3; cc++) {
+                const int rk = cc == 2 ? k : riz_t;
+                rare |= rk >= P.dbox[cc][0] && rk <= P.dbox[cc][1];
+            }
+        const bool cpml_here = col_cpml || qzl || qzh;
         // a sheet plane through this position (both sheet loops below act
         // only there)
         bool sheet_here = false;
@@ -449,6 +540,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
                 if (!S.nmask[q]) continue;
                 st<T>(S.es, q, S.sa[q] * ld<T>(S.es, q) + S.sb[q] * curl);
             }
+            if (rare) {
             // representative indices of this component
             const int ri = comp == 0 ? px + 1 : rix_t, rj = comp == 1 ? py + 1 : riy_t, rk = comp == 2 ? pz + 1 : riz_t;
             if (DRUDE && P.has_drude && in_box(P, comp, ri, rj, rk)) e = drude_update<T>(P, comp, px, py, pz, e, eold, gb, co);
@@ -519,10 +611,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 4 : (DRUDE ?
                     }
                 }
             }
+            }  // rare
 
             }  // cpml_split != 2
             // CPML on E, ref :6522-6670: Ex (y then z), Ey (x then z), Ez (x then y)
-            if (P.cpml_split == 1) {
+            if (P.cpml_split == 1 || !cpml_here) {
                 st<T>(Ec, c, e);
                 continue;
             }
