@@ -20,9 +20,11 @@ runs an independent replica (a single grid is not split across GPUs) and
 the value is the sum of the ranks' cell-updates over the slowest rank's
 time.  `e2e` times a complete K-step job through the C ABI from host
 buffers: model upload, K steps each followed by a device->host read of that
-step's port voltage, and the output files.  `--impl reference` times the
-CPU oracle (a C/OpenMP restatement of the reference's Fortran loop) on a
-256^3 sample of the same workload on all host threads.
+step's port voltage, and the output files (phases_s splits it into model
+set-up, steps and writes).  `--impl reference` times the CPU oracle (a
+C/OpenMP restatement of the reference's Fortran loop) on the same workload
+on all host threads: the GPU grid when host memory allows it, else the
+largest power-of-two fraction of it that fits (reference_grid).
 """
 import argparse
 import json
@@ -522,9 +524,12 @@ def ours(args):
         barrier()
         t0 = time.perf_counter()
         job = ab.Simulation(deck_text=deck_text(deck_k), ext_text=ext, bulk=host_bulk, outdir=etmp)
+        job.synchronize()
+        tc = time.perf_counter()
         for s in range(1, K + 1):
             job.run(1)
             job.probe("port_voltage", 0, first=s, n=1)
+        ts = time.perf_counter()
         job.write_outputs()
         t1 = time.perf_counter()
         h2d, d2h = job.transfer_bytes
@@ -532,7 +537,8 @@ def ours(args):
         wall = max_over_ranks(t1 - t0)
         e2e = {"value": round(world * cells * K / wall / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": round(h2d / K), "d2h_bytes_per_step": round(d2h / K),
-               "seconds": round(wall, 3), "steps": K}
+               "seconds": round(wall, 3), "steps": K,
+               "phases_s": {"create": round(tc - t0, 3), "steps": round(ts - tc, 3), "write": round(t1 - ts, 3)}}
 
     batched = None
     if not args.no_batch:
