@@ -330,7 +330,7 @@ __global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_const
 // per-step taps: plane sums (ref :7005-7190), phase-centre sample
 // (ref :8259-8290).  One block; plane sums reduce in a fixed tree order.
 template <typename T>
-__global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constant__ TapDev D,
+__global__ void __launch_bounds__(1024, 1) k_taps(const __grid_constant__ AemParams P, const __grid_constant__ TapDev D,
                        const __grid_constant__ FarFieldDev F, int counter, int steps) {
     counter = step_of(P, counter);
     __shared__ T red[4][1024];
@@ -340,15 +340,31 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
         const int nb = F.hi[b] - F.lo[b] + 1, nc = F.hi[c] - F.lo[c] + 1;
         const int i_lo = P.lo[a], i_hi = P.hi[a];
         T acc[4] = {zero<T>(), zero<T>(), zero<T>(), zero<T>()};
-        for (int q = tid; q < nb * nc; q += blockDim.x) {
-            int idx[3];
-            idx[b] = F.lo[b] + q % nb;
-            idx[c] = F.lo[c] + q / nb;
+        // a thread's points q = tid, tid + B, tid + 2B, ... in that order;
+        // the loads of four points are issued before their sums
+        constexpr int QU = 4;
+        const int nq = nb * nc;
+        for (int q0 = tid; q0 < nq; q0 += QU * blockDim.x) {
+            T ev[QU][2][2];
+#pragma unroll
+            for (int u = 0; u < QU; u++) {
+                const int q = q0 + u * blockDim.x;
+                if (q >= nq) continue;
+                int idx[3];
+                idx[b] = F.lo[b] + q % nb;
+                idx[c] = F.lo[c] + q / nb;
+                for (int side = 0; side < 2; side++) {
+                    idx[a] = side ? i_hi : i_lo;
+                    // the two transverse components: x plane (Ez, Ey), y (Ez, Ex), z (Ey, Ex)
+                    ev[u][side][0] = fget<T>(P, P.E[a == 2 ? 1 : 2], idx[0], idx[1], idx[2]);
+                    ev[u][side][1] = fget<T>(P, P.E[a == 0 ? 1 : 0], idx[0], idx[1], idx[2]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < QU; u++) {
+            if (q0 + u * (int)blockDim.x >= nq) continue;
             for (int side = 0; side < 2; side++) {
-                idx[a] = side ? i_hi : i_lo;
-                // the two transverse components: x plane (Ez, Ey), y (Ez, Ex), z (Ey, Ex)
-                const T e1 = fget<T>(P, P.E[a == 2 ? 1 : 2], idx[0], idx[1], idx[2]);
-                const T e2 = fget<T>(P, P.E[a == 0 ? 1 : 0], idx[0], idx[1], idx[2]);
+                const T e1 = ev[u][side][0], e2 = ev[u][side][1];
                 if (!P.kmax) {
                     T v;
                     if (a == 0) v = e1 * D.w1 - e2 * D.w2;
@@ -363,6 +379,7 @@ __global__ void k_taps(const __grid_constant__ AemParams P, const __grid_constan
                     acc[side] = acc[side] + te;
                     acc[2 + side] = acc[2 + side] + tm;
                 }
+            }
             }
         }
         for (int m = 0; m < 4; m++) red[m][tid] = acc[m];
