@@ -100,6 +100,8 @@ def load_library():
     lib.aem_design_set_eps.argtypes = [h, ctypes.c_void_p, ctypes.c_void_p]
     lib.aem_design_forward.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.aem_design_gradient.argtypes = [h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+    lib.aem_design_set_overlap.argtypes = [h, ctypes.c_int]
+    lib.aem_design_gradient_overlap.argtypes = [h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
     lib.aem_design_timing.argtypes = [h, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     lib.aem_design_get_field.argtypes = [h, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
     lib.aem_design_stream.argtypes = [h, ctypes.POINTER(ctypes.c_void_p)]

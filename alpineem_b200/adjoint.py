@@ -108,6 +108,23 @@ class Design:
                                                   float(scale)))
         return (ge, gs) if sigma else ge
 
+    def set_overlap(self, enable=True):
+        """Keep the spectra at the probe frequency of the forward E and of
+        the adjoint field on the design edges during gradient(), for
+        gradient_overlap()."""
+        self._check(self._lib.aem_design_set_overlap(self._h, 1 if enable else 0))
+
+    def gradient_overlap(self, scale=1.0):
+        """(dF/d eps_r, dF/d sigma) per design cell estimated from the two
+        spectra of the last gradient() alone: the frequency-domain overlap
+        of the reference's adjoint_optimization.py:121-134, restated for
+        this engine's adjoint field (a tone at the probe frequency assumed).
+        A consistency check on gradient(), not a replacement for it."""
+        ge = np.empty(self.shape, np.float32)
+        gs = np.empty(self.shape, np.float32)
+        self._check(self._lib.aem_design_gradient_overlap(self._h, ge.ctypes.data, gs.ctypes.data, float(scale)))
+        return ge, gs
+
     def timing(self):
         """(forward ms, gradient ms, forward launches, gradient launches) of
         the last calls, from CUDA events on the run's stream."""

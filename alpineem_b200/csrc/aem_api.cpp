@@ -451,6 +451,22 @@ int aem_design_gradient(aem_design* d, float* grad_eps, float* grad_sigma, doubl
     });
 }
 
+int aem_design_set_overlap(aem_design* d, int enable) {
+    if (!d) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        d->r->set_overlap(enable != 0);
+        return AEM_OK;
+    });
+}
+
+int aem_design_gradient_overlap(aem_design* d, float* grad_eps, float* grad_sigma, double scale) {
+    if (!d) return AEM_ERR_ARG;
+    return dguard(d, [&]() {
+        d->r->gradient_overlap(grad_eps, grad_sigma, scale);
+        return AEM_OK;
+    });
+}
+
 int aem_design_timing(aem_design* d, double ms[2], long long launches[2]) {
     if (!d || !ms || !launches) return AEM_ERR_ARG;
     d->r->timing(ms, launches);

@@ -80,6 +80,7 @@ struct DsnDev {
     double fdt2;   // 2 f dt
     double* dft;
     int acc_dft;
+    double* ov;    // [edge][4]: DFTs at the probe frequency of E^n and lE^n (overlap check), or null
 };
 
 template <typename R> __device__ __forceinline__ R dsn_div(R num, float dl);
@@ -489,8 +490,11 @@ __global__ void k_dsn_record(const __grid_constant__ AemParams P, const __grid_c
 // gradient sums of forward step n: lE^n at the design edges (the adjoint of
 // E^n = Ga E^{n-1} + Gb curl^n) times dE^n/dGa = E^{n-1} and
 // Gb dE^n/dGb = E^n - Ga E^{n-1}
+// With the overlap check on, also the DFTs at the probe frequency of E^n
+// (exp(-i w n dt), (pc, ps) = cos, sin of w n dt) and of lE^n (exp(+i w n dt)).
 template <typename R>
-__global__ void k_adj_grad(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int sn, int sm) {
+__global__ void k_adj_grad(const __grid_constant__ AemParams P, const __grid_constant__ DsnDev<R> D, int sn, int sm,
+                           double pc, double ps) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < D.nedge; q += (long long)gridDim.x * blockDim.x) {
         int px, py, pz;
         const int c = dsn_edge_pos(D, q, &px, &py, &pz);
@@ -498,6 +502,35 @@ __global__ void k_adj_grad(const __grid_constant__ AemParams P, const __grid_con
         const double en = (double)D.rec[sn * D.nedge + q], em = (double)D.rec[sm * D.nedge + q];
         D.A[q] += lam * em;
         D.B[q] += lam * (en - (double)D.ga[q] * em);
+        if (D.ov) {
+            double* o = D.ov + 4 * q;
+            o[0] += en * pc;
+            o[1] -= en * ps;
+            o[2] += lam * pc;
+            o[3] += lam * ps;
+        }
+    }
+}
+
+// The gradient sums A, B estimated from the two spectra alone, the
+// frequency-domain overlap of adjoint_optimization.py:121-134 restated for
+// this engine: for an adjoint field that is a tone at the probe frequency,
+// lE^n = Re(a exp(-i w n dt)) with a = 2 L / nwin (L its DFT over the nwin
+// steps), so A = sum lE^n E^{n-1} = Re(a z E) and
+// B = sum lE^n (E^n - Ga E^{n-1}) = Re(a (1 - Ga z) E), z = exp(-i w dt),
+// E the forward field's DFT.  (cw, sw) = cos, sin of w dt.
+template <typename R>
+__global__ void k_adj_overlap(const __grid_constant__ DsnDev<R> D, double* Ao, double* Bo, double nwin, double cw,
+                              double sw) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < D.nedge; q += (long long)gridDim.x * blockDim.x) {
+        const double* o = D.ov + 4 * q;
+        const double er = o[0], ei = o[1], ar = 2.0 * o[2] / nwin, ai = 2.0 * o[3] / nwin;
+        const double ga = (double)D.ga[q];
+        // a E
+        const double pr = ar * er - ai * ei, pi = ar * ei + ai * er;
+        // z = cw - i sw
+        Ao[q] = pr * cw + pi * sw;
+        Bo[q] = pr - ga * (pr * cw + pi * sw);
     }
 }
 
@@ -860,6 +893,8 @@ class DsnImpl : public DesignRun {
     void set_design(const float* eps, const float* sig) override;
     double forward(int checkpoint_every, double dft[2]) override;
     void gradient(float* geps, float* gsig, double scale) override;
+    void set_overlap(bool on) override;
+    void gradient_overlap(float* geps, float* gsig, double scale) override;
     void timing(double ms[2], long long launches[2]) const override {
         ms[0] = ms_[0]; ms[1] = ms_[1];
         launches[0] = launches_[0]; launches[1] = launches_[1];
@@ -919,6 +954,9 @@ class DsnImpl : public DesignRun {
     std::vector<std::pair<void*, size_t>> state_, adj_;  // forward state; adjoint state
     size_t state_bytes_ = 0;
     int steps_ = 0;
+    double* ov_buf_ = nullptr;  // overlap check: the two spectra per design edge
+    double* ov_ab_ = nullptr;   // overlap check: A, B estimated from them
+    bool ov_ready_ = false;
     bool probe_set_ = false, design_set_ = false;
     // checkpoints of the last forward()
     int K_ = 0, nseg_ = 0;
@@ -1126,7 +1164,14 @@ template <typename R>
 void DsnImpl<R>::adj_step(int n, int s0, const DsnDev<R>& D) {
     const dim3 blk(32, 8);
     if (n < steps_) {
-        k_adj_grad<R><<<egrid(D.nedge), 256, 0, st_>>>(P_, D, n - s0, n - 1 - s0);
+        double pc = 0.0, ps = 0.0;
+        if (D.ov) {
+            double ph = D_.fdt2 * (double)n;  // phase in half-turns
+            ph -= 2.0 * std::floor(0.5 * ph);
+            pc = std::cos(M_PI * ph);
+            ps = std::sin(M_PI * ph);
+        }
+        k_adj_grad<R><<<egrid(D.nedge), 256, 0, st_>>>(P_, D, n - s0, n - 1 - s0, pc, ps);
         launches_[1]++;
     }
     k_adj_ports_e<R><<<1, 256, 0, st_>>>(P_, S_, D, n);
@@ -1235,6 +1280,8 @@ void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     zero(adj_);
     DSN_CUDA(cudaMemsetAsync(D_.A, 0, D_.nedge * sizeof(double), st_));
     DSN_CUDA(cudaMemsetAsync(D_.B, 0, D_.nedge * sizeof(double), st_));
+    if (D_.ov) DSN_CUDA(cudaMemsetAsync(D_.ov, 0, 4 * D_.nedge * sizeof(double), st_));
+    ov_ready_ = false;
     DSN_CUDA(cudaEventRecord(ev_[0], st_));
     DSN_CUDA(cudaStreamWaitEvent(sb_, ev_[0], 0));
     launches_[1] = 0;
@@ -1293,6 +1340,36 @@ void DsnImpl<R>::gradient(float* geps, float* gsig, double scale) {
     float t = 0;
     DSN_CUDA(cudaEventElapsedTime(&t, ev_[0], ev_[1]));
     ms_[1] = t;
+    ov_ready_ = D_.ov != nullptr;
+}
+
+template <typename R>
+void DsnImpl<R>::set_overlap(bool on) {
+    if (on && !ov_buf_) {
+        ov_buf_ = alloc<double>(4 * (size_t)D_.nedge);
+        ov_ab_ = alloc<double>(2 * (size_t)D_.nedge);
+    }
+    D_.ov = on ? ov_buf_ : nullptr;
+    ov_ready_ = false;
+}
+
+template <typename R>
+void DsnImpl<R>::gradient_overlap(float* geps, float* gsig, double scale) {
+    if (!ov_ready_)
+        throw std::invalid_argument("design gradient: enable the overlap check, then run forward() and gradient()");
+    const double wdt = M_PI * D_.fdt2;  // w dt
+    DsnDev<R> Dv = D_;
+    Dv.A = ov_ab_;
+    Dv.B = ov_ab_ + D_.nedge;
+    k_adj_overlap<R><<<egrid(D_.nedge), 256, 0, st_>>>(D_, Dv.A, Dv.B, (double)(steps_ - 1), std::cos(wdt), std::sin(wdt));
+    const long long ncell = (long long)D_.n[0] * D_.n[1] * D_.n[2];
+    Scratch buf(2 * ncell * sizeof(float));
+    float* out = (float*)buf.p;
+    k_dsn_cellgrad<R><<<egrid(ncell), 256, 0, st_>>>(P_, Dv, out, out + ncell, scale);
+    DSN_CUDA(cudaGetLastError());
+    if (geps) DSN_CUDA(cudaMemcpyAsync(geps, out, ncell * sizeof(float), cudaMemcpyDefault, st_));
+    if (gsig) DSN_CUDA(cudaMemcpyAsync(gsig, out + ncell, ncell * sizeof(float), cudaMemcpyDefault, st_));
+    DSN_CUDA(cudaStreamSynchronize(st_));
 }
 
 template <typename R>

@@ -46,6 +46,14 @@ class DesignRun {
     // fastest; host or device pointers, either may be null), scaled by
     // `scale`; needs a forward() with checkpoints since the last set_design
     virtual void gradient(float* geps, float* gsig, double scale) = 0;
+    // Overlap check: with it on, gradient() also accumulates the DFTs at the
+    // probe frequency of the forward E and of the adjoint field on every
+    // design edge; gradient_overlap() then returns dF/d eps_r and dF/d sigma
+    // estimated from those two spectra alone (the frequency-domain overlap
+    // of adjoint_optimization.py:121-134, which assumes the adjoint field is
+    // a tone at that frequency), in gradient()'s layout and scale
+    virtual void set_overlap(bool on) = 0;
+    virtual void gradient_overlap(float* geps, float* gsig, double scale) = 0;
     // device time (ms) of the last forward() and gradient() calls, and the
     // kernel launches of each
     virtual void timing(double ms[2], long long launches[2]) const = 0;

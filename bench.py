@@ -99,6 +99,18 @@ def dram_traffic_ratio():
         return None
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def host_mem_available():
     """Bytes of host memory available (MemAvailable), or None."""
     try:
@@ -233,7 +245,8 @@ def reference_arm(args):
             "steps": steps, "warmup": warm, "ms_per_step": round(cells / (v * 1e6) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(n),
-            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "cpu_model": cpu_model()},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -556,7 +569,7 @@ def ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cn = min(args.cpu_baseline_n, reference_grid(args.n))
         v, threads, ccells = oracle_sample(cn, 1, args.cpu_steps)
-        cpu = {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
+        cpu = {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                "sample": "oracle (C/OpenMP restatement of the reference loop) on a %d^3 instance of the workload "
                          "(%d cells, same CPML, ellipsoids, port and 684 far-field angles), %d timed steps after 1 warm-up"
                          % (cn, ccells, args.cpu_steps)}

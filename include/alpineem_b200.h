@@ -321,6 +321,18 @@ int aem_design_forward(aem_design* d, int checkpoint_every, double* fom, double 
  * checkpointed aem_design_forward since the last aem_design_set_eps. */
 int aem_design_gradient(aem_design* d, float* grad_eps, float* grad_sigma, double scale);
 
+/* Overlap check (adjoint_optimization.py:121-134): the reference forms its
+ * gradient from the overlap, at one frequency, of the spectra of a forward
+ * and an adjoint run.  With enable != 0, aem_design_gradient also
+ * accumulates on every design edge the DFTs at the probe frequency of the
+ * forward E and of the adjoint field (32 B per edge), and
+ * aem_design_gradient_overlap returns the gradient estimated from those two
+ * spectra alone, assuming the adjoint field is a tone at that frequency, in
+ * aem_design_gradient's layout and scale.  Its distance from the exact
+ * gradient measures how far that assumption holds. */
+int aem_design_set_overlap(aem_design* d, int enable);
+int aem_design_gradient_overlap(aem_design* d, float* grad_eps, float* grad_sigma, double scale);
+
 /* Device time in ms of the last forward [0] and gradient [1] calls, and the
  * kernels each launched. */
 int aem_design_timing(aem_design* d, double ms[2], long long launches[2]);

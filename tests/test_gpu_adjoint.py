@@ -1,6 +1,7 @@
 """Design gradients (aem_design_*): the forward pass against the solver, the
 adjoint gradient against central finite differences, checkpoint segments,
-and the torch.autograd wrapper.
+the torch.autograd wrapper, and the frequency-domain overlap estimate of
+the reference's workflow as a consistency check.
 
 The workload is alpineem_b200.workloads.adjoint_probe at 48^3 (6-cell CPML,
 300 steps, a 10x10x6 design box of eps_r ~ U[1, 4], an Ez probe 8 cells
@@ -135,6 +136,49 @@ def test_checkpoint_segments_do_not_change_the_gradient(tmp_path, gpu_lib):
         grads.append(d.gradient())
     for g in grads[1:]:
         assert np.array_equal(g, grads[0])
+
+
+# The reference's gradient (adjoint_optimization.py:121-134) is the overlap
+# at one frequency of the spectra of a forward and an adjoint run.  Restated
+# for this engine it estimates the gradient from the DFTs at the probe
+# frequency of the forward E and of the adjoint field alone, assuming the
+# adjoint field is a tone there.  Measured on a B200 against the exact
+# gradient (rel. L2 over the design cells, eps / sigma): 300 steps 4.1e-2 /
+# 5.6e-2, 1000 steps 1.5e-2 / 0.14, 2000 steps 5.3e-3 / 0.12, 3000 steps
+# 5.1e-3 / 2.8e-2 (correlation 0.99999); the estimate approaches the exact
+# gradient as the window grows and the forward pulse has decayed.
+OVERLAP_TOL_EPS = 1e-2
+OVERLAP_TOL_SIGMA = 5e-2
+
+
+def test_overlap_estimate_agrees_with_gradient(tmp_path, gpu_lib):
+    path, lo, n, probe, freq, eps = _setup(tmp_path, steps=3000)
+    with _design(path, lo, n, probe, freq, 32) as d:
+        d.set_design(eps)
+        d.set_overlap(True)
+        d.forward(200)
+        ge, gs = d.gradient(sigma=True)
+        oe, os_ = d.gradient_overlap()
+    rel_e = np.linalg.norm(oe - ge) / np.linalg.norm(ge)
+    rel_s = np.linalg.norm(os_ - gs) / np.linalg.norm(gs)
+    assert rel_e <= OVERLAP_TOL_EPS, rel_e
+    assert rel_s <= OVERLAP_TOL_SIGMA, rel_s
+    assert np.corrcoef(oe.ravel(), ge.ravel())[0, 1] > 0.9999
+
+
+def test_overlap_needs_enabling(tmp_path, gpu_lib):
+    import alpineem_b200 as ab
+    path, lo, n, probe, freq, eps = _setup(tmp_path)
+    with _design(path, lo, n, probe, freq, 32) as d:
+        d.set_design(eps)
+        d.forward(100)
+        g = d.gradient()
+        with pytest.raises(ab.AemError, match="overlap"):
+            d.gradient_overlap()
+        # the check leaves the gradient itself unchanged
+        d.set_overlap(True)
+        d.forward(100)
+        assert np.array_equal(d.gradient(), g)
 
 
 def test_autograd_function(tmp_path, gpu_lib):
