@@ -19,6 +19,13 @@
   and the on-the-fly spectra at 256 frequencies against a float64 DFT of the
   run's own samples at <= 1e-12.
 
+* Batched constant-k sweep (workloads.kmax_batch): four of its 64 unit
+  cells (TE and TM, normal and oblique incidence, two depths), each with the
+  sweep's 16x16-patch sheet, slab and 128-frequency spectra, advanced
+  together by run_batch (graph replay, one stream each) for 320 steps;
+  every instance's four plane sums (TE and TM, reflected and transmitted)
+  against its own FP64 oracle run at <= 1e-4.
+
 With AEM_PRECISION_REPORT set to a file name, the errors against FP64 are
 appended to it as JSON lines, as in test_gpu_precision.py.
 """
@@ -137,3 +144,41 @@ def test_layered_slab_full_grid(tmp_path, oracle_bin, gpu_lib):
         assert len(f) == 256 and f[0] == 1e9 and f[-1] == 3e10
         ref = np.exp(-2j * np.pi * np.outer(f, m) * dt) @ g[k]
         assert np.linalg.norm(X - ref) <= 1e-12 * np.linalg.norm(ref), k
+
+
+def test_kmax_batch_instances(tmp_path, oracle_bin, gpu_lib):
+    import alpineem_b200 as ab
+    from alpineem_b200 import workloads
+    from alpineem_b200.deck import deck_text
+    steps, g = 320, 32
+    picks = (1, 2, 3, 4)  # TM 128, TE 128, TM 192 oblique, TE 128 oblique
+    # decks longer than the run: the oracle, cut short, dumps the raw sums
+    decks = workloads.kmax_batch(steps=steps + 64)
+    kinds = ("reflected", "transmitted", "reflected_tm", "transmitted_tm")
+    sims = []
+    try:
+        for q in picks:
+            d = tmp_path / ("gpu%d" % q)
+            d.mkdir()
+            sims.append(ab.Simulation(deck_text=deck_text(decks[q]), ext_text=workloads.KMAX_BATCH_EXT, kmax=True,
+                                      outdir=str(d)))
+        ab.run_batch(sims, steps, g)
+        got = [{k: sim.probe(k) for k in kinds} for sim in sims]
+    finally:
+        for sim in sims:
+            sim.close()
+    worst = 0.0
+    for q, gq in zip(picks, got):
+        od = tmp_path / ("o64_%d" % q)
+        od.mkdir()
+        _write(str(od), decks[q], workloads.KMAX_BATCH_EXT)
+        _run_oracle(oracle_bin["fdtd_oracle_kmax_f64"], str(od), max_steps=steps, dump_fields=False, dump_series=True)
+        o = {}
+        for k in kinds:
+            a = np.loadtxt(str(od / ("series_%s.txt" % k)))
+            o[k] = a[:, 0] + 1j * a[:, 1]
+        peak = max(np.linalg.norm(v) for v in o.values())
+        errs = {k: rel_l2(o[k], gq[k], floor=1e-3 * peak) for k in kinds}
+        _report({"deck": "kmax_batch_instance_%d_%d_steps" % (q, steps), "probe_rel_l2": max(errs.values())})
+        worst = max(worst, max(errs.values()))
+        assert max(errs.values()) <= TOL, (q, errs)
