@@ -100,8 +100,8 @@ __global__ void k_ff_base(const __grid_constant__ FarFieldDev F, int* kb, int* s
 }
 
 // One CTA per (face tile, group of F.group angles); see the file comment.
-// AW angles per warp (F.group = BIN_WARPS * AW).
-template <int AW>
+// AW angles per warp (F.group = BIN_WARPS * AW); TAIL: the run's last batch.
+template <int AW, bool TAIL>
 __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid_constant__ FarFieldDev F, int nlanes) {
     extern __shared__ __align__(16) float smem[];
     float* stage = smem;                                              // [2][32 cells][STAGE_STRIDE]
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid
                 wu[q] = w.wu;
                 ww[q] = w.ww;
                 on[q] = warp + BIN_WARPS * q < ng;  // warp-uniform
-                if (on[q] && ((unsigned)iu[q] > (unsigned)(HS - 32) || (unsigned)iw[q] > (unsigned)(HS - 32))) {
+                if (on[q] && ((unsigned)iu[q] > (unsigned)(HS - 33) || (unsigned)iw[q] > (unsigned)(HS - 33))) {
                     bad++;  // never: kb and hs come from the same expressions
                     on[q] = false;
                 }
@@ -223,6 +223,23 @@ __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid
                 float2* h = hist + (warp + BIN_WARPS * q) * 2 * HS;
                 h[iu[q] + lane] = pu[q];
                 h[HS + iw[q] + lane] = pw[q];
+            }
+            // the run's last batch: the last lane also adds the carried part
+            // of its step, w d(N), into the bin after its own (what a batch
+            // of one step with zero differences would add there)
+            if (TAIL && lane == nlanes - 1) {
+#pragma unroll
+                for (int q = 0; q < AW; q++) {
+                    if (!on[q]) continue;
+                    float2* h = hist + (warp + BIN_WARPS * q) * 2 * HS;
+                    float2 tu = h[iu[q] + nlanes], tw = h[HS + iw[q] + nlanes];
+                    tu.x += fmaf(wu[q], d[0], 0.0f);
+                    tu.y += fmaf(wu[q], d[1], 0.0f);
+                    tw.x += fmaf(ww[q], d[2], 0.0f);
+                    tw.y += fmaf(ww[q], d[3], 0.0f);
+                    h[iu[q] + nlanes] = tu;
+                    h[HS + iw[q] + nlanes] = tw;
+                }
             }
         }
         if (v + 1 < nv) store_row(stage + ((v + 1) & 1) * STAGE_FLOATS, pre);
@@ -306,9 +323,10 @@ __global__ void k_ff_carry(const __grid_constant__ FarFieldDev F, int carry) {
 }
 
 template <int AW>
-void bin_launch(const FarFieldDev& F, int nlanes, cudaStream_t s) {
+void bin_launch(const FarFieldDev& F, int nlanes, bool tail, cudaStream_t s) {
     dim3 grid((unsigned)F.ngrp, (unsigned)F.ntiles);
-    k_ff_bin_tiles<AW><<<grid, BIN_WARPS * 32, ff_tiles_smem(F), s>>>(F, nlanes);
+    if (tail) k_ff_bin_tiles<AW, true><<<grid, BIN_WARPS * 32, ff_tiles_smem(F), s>>>(F, nlanes);
+    else k_ff_bin_tiles<AW, false><<<grid, BIN_WARPS * 32, ff_tiles_smem(F), s>>>(F, nlanes);
 }
 
 }  // namespace
@@ -319,9 +337,12 @@ size_t ff_tiles_smem(const FarFieldDev& F) {
 
 void ff_tiles_prepare() {
     const int lim = 200 * 1024;
-    cudaFuncSetAttribute(k_ff_bin_tiles<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_ff_bin_tiles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_ff_bin_tiles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_ff_bin_tiles<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 int launch_ff_base(const FarFieldDev& F, int* kb, int* span, cudaStream_t s) {
@@ -330,12 +351,13 @@ int launch_ff_base(const FarFieldDev& F, int* kb, int* span, cudaStream_t s) {
     return 1;
 }
 
-int launch_ff_bin_tiles(const AemParams& P, const FarFieldDev& F, int n0, int nlanes, int carry, cudaStream_t s) {
+int launch_ff_bin_tiles(const AemParams& P, const FarFieldDev& F, int n0, int nlanes, int carry, cudaStream_t s,
+                        bool tail) {
     if (!F.nvc || !F.ntiles || nlanes <= 0) return 0;
     const int aw = F.group / BIN_WARPS;
-    if (aw >= 4) bin_launch<4>(F, nlanes, s);
-    else if (aw == 2) bin_launch<2>(F, nlanes, s);
-    else bin_launch<1>(F, nlanes, s);
+    if (aw >= 4) bin_launch<4>(F, nlanes, tail, s);
+    else if (aw == 2) bin_launch<2>(F, nlanes, tail, s);
+    else bin_launch<1>(F, nlanes, tail, s);
     k_ff_reduce<<<(unsigned)F.nangc, 256, 0, s>>>(P, F, n0, nlanes);
     int n = 2;
     if (carry > 0) {

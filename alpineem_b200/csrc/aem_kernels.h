@@ -124,8 +124,11 @@ int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStr
 // deterministic tiled binning (aem_ffbin.cu): bin `nlanes` steps starting at
 // n0 (the differences in slots 1..nlanes, the step before in slot 0), add
 // the windows to the FP64 accumulators in a fixed order, then move slot
-// `carry` to slot 0 for the next batch (carry < 0: no move)
-int launch_ff_bin_tiles(const AemParams& P, const FarFieldDev& F, int n0, int nlanes, int carry, cudaStream_t s);
+// `carry` to slot 0 for the next batch (carry < 0: no move).  tail: the
+// run's last batch, whose last lane also bins the carried part of the final
+// step (the windows need FF_TB + 1 bins beyond the span)
+int launch_ff_bin_tiles(const AemParams& P, const FarFieldDev& F, int n0, int nlanes, int carry, cudaStream_t s,
+                        bool tail = false);
 // window bases kb and the largest window span over all (tile, angle)
 int launch_ff_base(const FarFieldDev& F, int* kb, int* span, cudaStream_t s);
 size_t ff_tiles_smem(const FarFieldDev& F);  // dynamic shared bytes of one binning CTA

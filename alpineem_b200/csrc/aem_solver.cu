@@ -557,7 +557,7 @@ void Solver::setup_farfield() {
             AEM_CUDA(cudaStreamSynchronize(stream_));
             AEM_CUDA(cudaGetLastError());
             F.kb = kb_d;
-            F.hs = span + FF_TB;  // offsets base .. base+span, plus the 32 lanes
+            F.hs = span + FF_TB + 1;  // offsets base .. base+span, plus the 32 lanes and the final step's carry
             // angles per CTA: 8 warps x AW, two CTAs per SM
             const size_t stage = (size_t)2 * FF_TILE * (4 * 33 + 1) * sizeof(float);
             const size_t per = (size_t)2 * F.hs * 2 * sizeof(float);
@@ -895,7 +895,8 @@ void Solver::step(int counter) {
     if (FF_.tb > 1) {
         // differences go to slot counter - ff_n0_ + 1; a full batch is binned at once
         phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, counter - ff_n0_ + 1, stream_); });
-        if (counter - ff_n0_ + 1 == FF_.tb) flush_farfield(counter);
+        if (counter == m_.d.steps && !P_.dstep) flush_farfield_last(counter);
+        else if (counter - ff_n0_ + 1 == FF_.tb) flush_farfield(counter);
     } else {
         phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, 0, stream_); });
         phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin(P_, FF_, counter, stream_); });
@@ -913,6 +914,16 @@ void Solver::flush_farfield(int last) {
         phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, nt, stream_); });
     }
     ff_n0_ = last + 1;
+}
+
+// the deck's last step, run eagerly: its batch and the carried-over part of
+// that step in one launch (a separate one-lane launch costs as much as a
+// full batch); ff_n0_ then points past the tail, as flush_farfield_tail
+// leaves it
+void Solver::flush_farfield_last(int last) {
+    const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
+    phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, -1, stream_, true); });
+    ff_n0_ = m_.d.steps + 2;
 }
 
 // after the deck's last step: the carried-over part of that step, binned as
