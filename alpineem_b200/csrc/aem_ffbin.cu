@@ -224,21 +224,53 @@ __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid
                 h[iu[q] + lane] = pu[q];
                 h[HS + iw[q] + lane] = pw[q];
             }
-            // the run's last batch: the last lane also adds the carried part
-            // of its step, w d(N), into the bin after its own (what a batch
-            // of one step with zero differences would add there)
-            if (TAIL && lane == nlanes - 1) {
+        }
+        // the run's last batch: the carried part of the final step, w d(N),
+        // of every cell of the row goes into the bin after that step's own
+        // (what a batch of one step with zero differences would add there).
+        // Lane u takes cell u; the cells of a row reach each bin in one
+        // contiguous run (the offset is monotonic along the row), so a
+        // masked shuffle sum gathers each run onto its first lane, which
+        // alone adds it to the histogram.
+        if (TAIL) {
+            const bool cell = lane < nu;
+            const float* c = cur + lane * STAGE_STRIDE;
+            float dn[4];
 #pragma unroll
-                for (int q = 0; q < AW; q++) {
-                    if (!on[q]) continue;
-                    float2* h = hist + (warp + BIN_WARPS * q) * 2 * HS;
-                    float2 tu = h[iu[q] + nlanes], tw = h[HS + iw[q] + nlanes];
-                    tu.x += fmaf(wu[q], d[0], 0.0f);
-                    tu.y += fmaf(wu[q], d[1], 0.0f);
-                    tw.x += fmaf(ww[q], d[2], 0.0f);
-                    tw.y += fmaf(ww[q], d[3], 0.0f);
-                    h[iu[q] + nlanes] = tu;
-                    h[HS + iw[q] + nlanes] = tw;
+            for (int m = 0; m < 4; m++) dn[m] = cell ? c[m * 33 + nlanes] : 0.0f;
+            const float uf = (float)(u0 + lane);
+#pragma unroll
+            for (int q = 0; q < AW; q++) {
+                if (warp + BIN_WARPS * q >= ng) continue;  // warp-uniform
+                const BinW w = ff_binw(fmaf(Ku[q], uf, trow[q]));
+                int key[2] = {cell ? w.ku - base[q] + nlanes : -1 - lane, cell ? w.kw - base[q] + nlanes : -1 - lane};
+                float2 val[2] = {make_float2(fmaf(w.wu, dn[0], 0.0f), fmaf(w.wu, dn[1], 0.0f)),
+                                 make_float2(fmaf(w.ww, dn[2], 0.0f), fmaf(w.ww, dn[3], 0.0f))};
+#pragma unroll
+                for (int h2 = 0; h2 < 2; h2++) {
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const int ko = __shfl_down_sync(0xffffffffu, key[h2], off);
+                        const float vx = __shfl_down_sync(0xffffffffu, val[h2].x, off);
+                        const float vy = __shfl_down_sync(0xffffffffu, val[h2].y, off);
+                        if (lane + off < 32 && ko == key[h2]) {
+                            val[h2].x += vx;
+                            val[h2].y += vy;
+                        }
+                    }
+                    const int kp = __shfl_up_sync(0xffffffffu, key[h2], 1);
+                    const bool head = cell && (lane == 0 || kp != key[h2]);
+                    if (head) {
+                        if ((unsigned)key[h2] > (unsigned)(HS - 1)) {
+                            bad++;  // never: hs holds the span, the 32 lanes and this bin
+                        } else {
+                            float2* hh = hist + (warp + BIN_WARPS * q) * 2 * HS + h2 * HS;
+                            float2 t = hh[key[h2]];
+                            t.x += val[h2].x;
+                            t.y += val[h2].y;
+                            hh[key[h2]] = t;
+                        }
+                    }
                 }
             }
         }
