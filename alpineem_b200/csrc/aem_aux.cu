@@ -233,95 +233,25 @@ __global__ void k_ff_currents(const __grid_constant__ AemParams P, const __grid_
         }
         T* cur = reinterpret_cast<T*>(F.cur[a][s]);
         const long long n = F.face_n[a];
-        if constexpr (sizeof(T) == sizeof(float)) {
-            if (F.dtile) {
-                // tiled difference buffer of the batched binning: tile of
-                // (u, v), slot `slot` (1-based step of the batch)
-                const int u = (int)(q % nb), vv = (int)(q / nb);
-                const long long tile = F.tile0[2 * a + s] + (u >> 5) + (long long)(vv >> 5) * F.tiles_u[a];
-                float* dt = F.dtile + (tile * FF_SLOTS + slot) * 4 * 1024 + ((vv & 31) << 5) + (u & 31);
-                for (int m = 0; m < 4; m++) {
-                    const float nv = v[m];
-                    dt[m * 1024] = nv - cur[m * n + q];  // M - M_o, ref :7667
-                    cur[m * n + q] = nv;
-                }
-                continue;
-            }
-        }
-        T* dif = reinterpret_cast<T*>(F.dbuf[a][s]);
+        // tiled difference buffer of the batched binning: tile of (u, v),
+        // slot `slot` (1-based step of the batch); a complex run keeps the
+        // imaginary parts in a second plane after the real ones
+        const int u = (int)(q % nb), vv = (int)(q / nb);
+        const long long tile = F.tile0[2 * a + s] + (u >> 5) + (long long)(vv >> 5) * F.tiles_u[a];
+        float* dt = F.dtile + (tile * FF_SLOTS + slot) * 4 * 1024 + ((vv & 31) << 5) + (u & 31);
         for (int m = 0; m < 4; m++) {
-            const T nv = unphase<T>(P, F, v[m], i, j, k, a);
-            dif[(long long)m * n + q] = nv - cur[m * n + q];  // M - M_o, ref :7667
-            cur[m * n + q] = nv;
-        }
-    }
-}
-
-template <typename T>
-__device__ inline void atomic_add(T* p, T v);
-template <>
-__device__ inline void atomic_add<float>(float* p, float v) { atomicAdd(p, v); }
-template <>
-__device__ inline void atomic_add<cf>(cf* p, cf v) { atomicAdd(&p->x, v.x); atomicAdd(&p->y, v.y); }
-
-// retarded-time binning, ref :7660-7730 (mirrored form :7958-8230 with the
-// image position and sign factors)
-template <typename T>
-__global__ void k_ff_bin(const __grid_constant__ AemParams P, const __grid_constant__ FarFieldDev F, int counter) {
-    counter = step_of(P, counter);
-    const long long cells = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]);
-    const long long tot = cells * F.nang;
-    T* UW = reinterpret_cast<T*>(F.UW);
-    const long long L = F.len;
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < tot; g += (long long)gridDim.x * blockDim.x) {
-        const int ang = (int)(g / cells);
-        long long r = g % cells;
-        int a = 0;
-        while (r >= 2 * F.face_n[a]) { r -= 2 * F.face_n[a]; a++; }
-        const int s = (int)(r / F.face_n[a]);
-        const long long q = r % F.face_n[a];
-        const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
-        const int nb = F.hi[b] - F.lo[b] + 1;
-        int idx[3];
-        idx[a] = s ? F.hi[a] : F.lo[a];
-        idx[b] = F.lo[b] + (int)(q % nb);
-        idx[c] = F.lo[c] + (int)(q / nb);
-        const T* dif = reinterpret_cast<const T*>(F.dbuf[a][s]);
-        const long long n = F.face_n[a];
-        T d[4];
-        for (int m = 0; m < 4; m++) d[m] = dif[(long long)m * n + q];
-        // component slots: W = 0..2, U = 3..5; (M1, M2, J1, J2) per face normal
-        const int u1 = a == 0 ? 4 : 3, u2 = a == 2 ? 4 : 5, w1 = a == 0 ? 1 : 0, w2 = a == 2 ? 1 : 2;
-        const float* A = F.ang + 4 * ang;  // sin(th), cos(th), sin(ph), cos(ph)
-        const float fac = F.fac[a];
-        for (int pass = 0; pass <= F.mirror; pass++) {
-            float pos[3];
-            float sm[4] = {1.0f, 1.0f, 1.0f, 1.0f};
-            for (int e = 0; e < 3; e++) {
-                pos[e] = (float)(idx[e]);
-                if (pass) pos[e] = (float)idx[e] * (1.0f - F.use_mir[e]) + (F.mir_off[e] - (float)idx[e]) * F.use_mir[e];
+            if constexpr (sizeof(T) == sizeof(float)) {
+                const float nv = v[m];
+                dt[m * 1024] = nv - cur[m * n + q];  // M - M_o, ref :7667
+                cur[m * n + q] = nv;
+            } else {
+                const T nv = unphase<T>(P, F, v[m], i, j, k, a);  // ref :7202-7331
+                const T df = nv - cur[m * n + q];
+                const long long plane = (long long)F.ntiles * FF_SLOTS * 4 * 1024;
+                dt[m * 1024] = df.x;
+                dt[plane + m * 1024] = df.y;
+                cur[m * n + q] = nv;
             }
-            if (pass) {
-                const int mc1 = a == 0 ? 1 : 0, mc2 = a == 2 ? 1 : 2;  // tangential axes of this face
-                sm[0] = F.M_mir[mc1]; sm[1] = F.M_mir[mc2]; sm[2] = F.J_mir[mc1]; sm[3] = F.J_mir[mc2];
-            }
-            const float proj = (pos[0] - (float)F.ic) * P.del[0] * A[0] * A[3] + (pos[1] - (float)F.jc) * P.del[1] * A[0] * A[2] +
-                               (pos[2] - (float)F.kc) * P.del[2] * A[1];
-            const float tf = (F.r_relay - proj) / F.c_dt;
-            float t = (float)counter + 0.5f + tf - 1.0f;
-            int ii = (int)t;
-            float wt = t - (float)ii;
-            atomic_add<T>(&UW[(u1 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[0] * sm[0]));
-            atomic_add<T>(&UW[(u1 * F.nang + ang) * L + ii], wt * fac * (d[0] * sm[0]));
-            atomic_add<T>(&UW[(u2 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[1] * sm[1]));
-            atomic_add<T>(&UW[(u2 * F.nang + ang) * L + ii], wt * fac * (d[1] * sm[1]));
-            t = (float)counter + tf - 1.0f;
-            ii = (int)t;
-            wt = t - (float)ii;
-            atomic_add<T>(&UW[(w1 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[2] * sm[2]));
-            atomic_add<T>(&UW[(w1 * F.nang + ang) * L + ii], wt * fac * (d[2] * sm[2]));
-            atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii - 1], (1.0f - wt) * fac * (d[3] * sm[3]));
-            atomic_add<T>(&UW[(w2 * F.nang + ang) * L + ii], wt * fac * (d[3] * sm[3]));
         }
     }
 }
@@ -552,16 +482,6 @@ int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaS
     int blocks = (int)((tot + 255) / 256 < 148 * 16 ? (tot + 255) / 256 : 148 * 16);
     if (P.kmax) k_ff_currents<cf><<<blocks, 256, 0, s>>>(P, F, slot);
     else k_ff_currents<float><<<blocks, 256, 0, s>>>(P, F, slot);
-    return 1;
-}
-int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s) {
-    // per-step binning with float atomics: the constant-k (complex) path;
-    // FP32 runs use the tiled batch binning of aem_ffbin.cu
-    if (!F.nang || !P.kmax) return 0;
-    long long tot = 2 * (F.face_n[0] + F.face_n[1] + F.face_n[2]) * F.nang;
-    if (tot == 0) return 0;
-    int blocks = (int)((tot + 255) / 256 < 148 * 32 ? (tot + 255) / 256 : 148 * 32);
-    k_ff_bin<cf><<<blocks, 256, 0, s>>>(P, F, counter);
     return 1;
 }
 int launch_taps(const AemParams& P, const TapDev& D, const FarFieldDev& F, int counter, int steps, cudaStream_t s) {

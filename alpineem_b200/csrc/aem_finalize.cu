@@ -33,8 +33,9 @@ using cplx = std::complex<float>;
 // operation order: Wt = (wx c1) c2 + (wy c1) s2 - wz s1, Wp = (-1 wx) s2 +
 // wy c2 (U likewise), Et = (-1 eta) Wt - Up, Ep = (-1 eta) Wp + Ut.  The
 // angle's cosines and sines come from the host.
-// The accumulators A are FP64 on the FP32 path (rounded to FP32 here, the
-// precision the reference's U/W arrays hold) and complex64 for kmax.
+// The accumulators are FP64 (rounded to FP32 here, the precision the
+// reference's U/W arrays hold); a constant-k run's real and imaginary
+// planes are first joined into complex64 (k_ff_join).
 __device__ inline float to_v(double x, float) { return (float)x; }
 __device__ inline cf to_v(cf x, cf) { return x; }
 template <typename V, typename A>
@@ -51,6 +52,12 @@ __device__ inline void ff_pol(const A* uw, long long stride, long long j, const 
     Et = me * Wt - Up;
     Ep = me * Wp + Ut;
 }
+// the real and imaginary FP64 planes of a constant-k run -> complex64
+__global__ void k_ff_join(const double* re, const double* im, cf* out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = cf{(float)re[i], (float)im[i]};
+}
+
 __device__ inline bool nz(float v) { return v != 0.0f; }
 __device__ inline bool nz(cf v) { return v.x != 0.0f || v.y != 0.0f; }
 
@@ -217,10 +224,14 @@ void Solver::finalize_and_write() {
         void* d_eph = alloc((size_t)nff * T * es_);
         AEM_CUDA(cudaMemcpyAsync(d_trig, trig.data(), trig.size() * sizeof(float), cudaMemcpyHostToDevice, stream_));
         AEM_CUDA(cudaMemcpyAsync(d_canon, canon.data(), canon.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
-        if (K)
-            k_ff_out<cf, cf><<<nff, 256, 0, stream_>>>((const cf*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig, eta,
-                                                       d_canon, (cf*)d_eth, (cf*)d_eph, d_time);
-        else
+        if (K) {
+            const long long nuw = (long long)6 * nff * L;
+            cf* d_uw = (cf*)alloc((size_t)nuw * sizeof(cf));
+            const double* uw = (const double*)FF_.UW;
+            k_ff_join<<<(unsigned)std::min<long long>((nuw + 255) / 256, 148 * 8), 256, 0, stream_>>>(uw, uw + nuw, d_uw, nuw);
+            k_ff_out<cf, cf><<<nff, 256, 0, stream_>>>(d_uw, nff, (long long)L, d.len_ff, T, d_trig, eta, d_canon,
+                                                       (cf*)d_eth, (cf*)d_eph, d_time);
+        } else
             k_ff_out<float, double><<<nff, 256, 0, stream_>>>((const double*)FF_.UW, nff, (long long)L, d.len_ff, T, d_trig,
                                                               eta, d_canon, (float*)d_eth, (float*)d_eph, d_time);
         AEM_CUDA(cudaGetLastError());

@@ -41,15 +41,14 @@ struct FarFieldDev {
     float wall_lo[3], wall_hi[3];
     const float* ang;           // per angle: sin(th), cos(th), sin(ph), cos(ph)
     void* cur[3][2];            // per face normal / side: the 4 current components of the last step
-    void* dbuf[3][2];           // per face (constant-k path): (new - old) of the 4 components, [comp][cell]
     long long face_n[3];        // cells per face of that normal
-    void* UW;                   // [6][nang][len]: Wx,Wy,Wz,Ux,Uy,Uz (FP64 sums on the FP32 path, complex64 for kmax)
+    void* UW;                   // [6][nang][len] FP64: Wx,Wy,Wz,Ux,Uy,Uz (kmax: a real plane, then an imaginary one)
     int mirror;                 // image-ground-plane pass
     float mir_off[3], use_mir[3], M_mir[3], J_mir[3];
     float kc3[3];               // kmax: k_count for Bloch-phase removal
-    // time-batched binning (FP32 path): the differences of tb steps are kept
-    // and binned together; tb == 1 (constant-k runs) bins every step with
-    // the per-contribution kernel and float atomics
+    // time-batched binning: the differences of tb steps are kept and binned
+    // together; constant-k runs bin their real and imaginary parts as two
+    // planes of dtile and UW, each as an FP32 run's
     int tb;
     int nvang;                  // virtual angles: nang * (1 + mirror), image pass second
     int tiles_u[3], tiles_v[3]; // 32x32 tiles per face of each normal
@@ -120,7 +119,6 @@ int launch_update_e(const AemParams& P, int counter, cudaStream_t s);
 int launch_ports_h(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
 int launch_ports_e(const AemParams& P, const PortSet& ps, int counter, cudaStream_t s);
 int launch_ff_currents(const AemParams& P, const FarFieldDev& F, int slot, cudaStream_t s);
-int launch_ff_bin(const AemParams& P, const FarFieldDev& F, int counter, cudaStream_t s);
 // deterministic tiled binning (aem_ffbin.cu): bin `nlanes` steps starting at
 // n0 (the differences in slots 1..nlanes, the step before in slot 0), add
 // the windows to the FP64 accumulators in a fixed order, then move slot

@@ -474,9 +474,9 @@ void Solver::setup_farfield() {
         ang[4 * q + 3] = std::cos(d.ff_phi[q]);
     }
     F.ang = (const float*)upload(ang);
-    // accumulators: FP64 on the FP32 path (deterministic ordered sums),
-    // complex64 on the constant-k path
-    F.UW = alloc((size_t)6 * F.nang * F.len * (d.kmax ? es_ : sizeof(double)));
+    // accumulators: FP64 (deterministic ordered sums); a constant-k run
+    // keeps a real and an imaginary plane
+    F.UW = alloc((size_t)6 * F.nang * F.len * sizeof(double) * (d.kmax ? 2 : 1));
     F.err = (int*)alloc(sizeof(int));
 
     // retarded-time offset of face cell (u, v) for virtual angle va (image
@@ -526,10 +526,10 @@ void Solver::setup_farfield() {
             ff_canon_[q] = first.emplace(key, q).first->second;
         }
     }
-    // FP32 runs: batches of FF_TB steps, binned deterministically over 32x32
-    // face tiles (aem_ffbin.cu); constant-k runs bin every step
-    F.tb = d.kmax ? 1 : FF_TB;
-    if (F.tb > 1) {
+    // batches of FF_TB steps, binned deterministically over 32x32 face tiles
+    // (aem_ffbin.cu); a constant-k run bins its real and imaginary planes
+    F.tb = FF_TB;
+    {
         F.kf = (const float*)upload(kf);
         F.tile0[0] = 0;
         for (int f = 0; f < 6; f++) F.tile0[f + 1] = F.tile0[f] + (long long)F.tiles_u[f >> 1] * F.tiles_v[f >> 1];
@@ -609,19 +609,14 @@ void Solver::setup_farfield() {
             F.nangc = (int)clist.size() / 4;
             F.clist = (const int*)upload(clist);
             F.crange = (const int*)upload(crange);
-            F.dtile = (float*)alloc((size_t)F.ntiles * FF_SLOTS * 4 * 1024 * sizeof(float));
+            F.dtile = (float*)alloc((size_t)F.ntiles * FF_SLOTS * 4 * 1024 * sizeof(float) * (d.kmax ? 2 : 1));
             ff_part_bytes_ = (size_t)F.ntiles * F.nvc * 4 * F.hs * sizeof(float);
             ff_tiles_prepare();
         }
-    } else {
-        for (int q = 0; q < F.nang; q++) ff_canon_[q] = q;  // the per-step path bins every angle
     }
     for (int a = 0; a < 3; a++)
         for (int s = 0; s < 2; s++)
-            if (F.has[a]) {
-                F.cur[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
-                if (F.tb == 1) F.dbuf[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
-            }
+            if (F.has[a]) F.cur[a][s] = alloc((size_t)F.face_n[a] * 4 * es_);
 }
 
 void Solver::setup_taps() {
@@ -892,14 +887,11 @@ void Solver::step(int counter) {
         phase(AEM_PHASE_UPDATE_E, [&] { return launch_update_e(P_, counter, stream_); });
         phase(AEM_PHASE_PORTS, [&] { return launch_ports_e(P_, PS_, counter, stream_); });
     }
-    if (FF_.tb > 1) {
+    {
         // differences go to slot counter - ff_n0_ + 1; a full batch is binned at once
         phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, counter - ff_n0_ + 1, stream_); });
         if (counter == m_.d.steps && !P_.dstep) flush_farfield_last(counter);
         else if (counter - ff_n0_ + 1 == FF_.tb) flush_farfield(counter);
-    } else {
-        phase(AEM_PHASE_FF_CURRENTS, [&] { return launch_ff_currents(P_, FF_, 0, stream_); });
-        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin(P_, FF_, counter, stream_); });
     }
     phase(AEM_PHASE_TAPS, [&] { return launch_taps(P_, TP_, FF_, counter, m_.d.steps, stream_); });
     if (full_.f[0]) full_tap(counter);
@@ -909,11 +901,22 @@ void Solver::step(int counter) {
 // moves to slot 0, where the next batch takes its carried-over part
 void Solver::flush_farfield(int last) {
     if (last < ff_n0_) return;  // nothing buffered (and the tail, if done, stays done)
-    if (FF_.tb > 1) {
-        const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
-        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, nt, stream_); });
-    }
+    const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
+    bin_farfield(n0, nt, nt, false);
     ff_n0_ = last + 1;
+}
+
+// the binning launches of one batch: the real plane, and for a constant-k
+// run the imaginary plane (its differences and accumulators follow the
+// real ones)
+void Solver::bin_farfield(int n0, int nt, int carry, bool tail) {
+    phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, carry, stream_, tail); });
+    if (m_.d.kmax) {
+        FarFieldDev Fi = FF_;
+        Fi.dtile = FF_.dtile ? FF_.dtile + (size_t)FF_.ntiles * FF_SLOTS * 4 * 1024 : nullptr;
+        Fi.UW = (double*)FF_.UW + (size_t)6 * FF_.nang * FF_.len;
+        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, Fi, n0, nt, carry, stream_, tail); });
+    }
 }
 
 // the deck's last step, run eagerly: its batch and the carried-over part of
@@ -922,7 +925,7 @@ void Solver::flush_farfield(int last) {
 // leaves it
 void Solver::flush_farfield_last(int last) {
     const int n0 = ff_n0_, nt = last - ff_n0_ + 1;
-    phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, n0, nt, -1, stream_, true); });
+    bin_farfield(n0, nt, -1, true);
     ff_n0_ = m_.d.steps + 2;
 }
 
@@ -931,8 +934,8 @@ void Solver::flush_farfield_last(int last) {
 // it, so this runs once (a checkpoint carries ff_n0_)
 void Solver::flush_farfield_tail() {
     const int steps = m_.d.steps;
-    if (FF_.tb > 1 && done_ == steps && ff_n0_ == steps + 1) {
-        phase(AEM_PHASE_FF_BIN, [&] { return launch_ff_bin_tiles(P_, FF_, steps + 1, 1, -1, stream_); });
+    if (done_ == steps && ff_n0_ == steps + 1) {
+        bin_farfield(steps + 1, 1, -1, false);
         ff_n0_ = steps + 2;
     }
 }

@@ -127,6 +127,7 @@ class Solver {
     void flush_farfield(int last);
     void flush_farfield_tail();
     void flush_farfield_last(int last);
+    void bin_farfield(int n0, int nt, int carry, bool tail);
     bool graph_ready(int g) const;  // can a g-step graph chunk start at the next step?
     void full_tap(int counter);
     void full_drain(int b);
