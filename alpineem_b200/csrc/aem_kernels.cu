@@ -64,9 +64,10 @@ constexpr int UPD_ZCH = 16, UPD_TY = 8;
 // flag per position, made of a column test done once and a plane test
 // done per plane.  E(k+1) stays in registers as the next plane's E(k).
 // The complex instantiation runs at 3 CTAs per SM (no spills).
-template <typename T>
+template <typename T, bool SHEETS>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
+    const int NS = SHEETS ? P.nsheet : 0;  // decks without sheets compile the sheet code out
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     // H is updated on reference indices 1..N-1 of every axis (all positions
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
     // rare corrections that this column can take: an x or y sheet plane
     // through it, a TF/SF x or y face, the constant-k source plane
     bool col_rare = false;
-    for (int s = 0; s < P.nsheet; s++)
+    for (int s = 0; s < NS; s++)
         col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
     if (sizeof(T) == sizeof(float) && P.tfsf_on)
         col_rare |= (!P.per[0] && (i == P.lo[0] - 1 || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] - 1 || j == P.hi[1]));
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
         const T ez_ip = ld_up<T>(P, Ez, c + offx, wx, 0);
         const T ez_jp = ld_up<T>(P, Ez, c + offy, wy, 1);
         bool rare = col_rare;
-        for (int s = 0; s < P.nsheet; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
+        for (int s = 0; s < NS; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
         if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] - 1 || k == P.hi[2]);
         if (sizeof(T) != sizeof(float) && P.kmax_mode_TE) rare |= P.kmax_src_axis == 2 && k == P.k_pl_H;
 
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
 
         if (rare) {
         // Smith-Maloney sheets, ref :4486-4554
-        for (int s = 0; s < P.nsheet; s++) {
+        for (int s = 0; s < NS; s++) {
             const AemSheetPlane& S = P.sheet[s];
             const int pn = S.axis == 0 ? px : S.axis == 1 ? py : pz;
             if (pn != S.pos) continue;  // S.pos is a storage position
@@ -379,9 +380,10 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
 // from the previous plane (FP32; the complex kernel reloads them and runs
 // 3 CTAs per SM without Drude poles, which overlaps better in a batch of
 // constant-k runs: 0.79 s against 1.00 s at 2 CTAs for 64 unit cells).
-template <typename T, bool DRUDE>
+template <typename T, bool DRUDE, bool SHEETS>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ? 2 : 3)) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
+    const int NS = SHEETS ? P.nsheet : 0;  // decks without sheets compile the sheet code out
     const int px = blockIdx.x * 32 + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     __shared__ CoefTabs Tb;
@@ -420,7 +422,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
     // through it, a TF/SF x or y face, the constant-k source plane, a
     // Drude box over it
     bool col_rare = false;
-    for (int s = 0; s < P.nsheet; s++)
+    for (int s = 0; s < NS; s++)
         col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
     if (sizeof(T) == sizeof(float) && P.tfsf_on)
         col_rare |= (!P.per[0] && (i == P.lo[0] || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] || j == P.hi[1]));
@@ -487,7 +489,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
         idy_prev = idy;
         have = sizeof(T) == sizeof(float) && !unavg;  // the ids of this plane were read (FP32 only, as in H)
         bool rare = col_rare;
-        for (int s = 0; s < P.nsheet; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
+        for (int s = 0; s < NS; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
         if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] || k == P.hi[2]);
         if (sizeof(T) != sizeof(float) && P.kmax_mode_TM)
             rare |= P.kmax_src_axis == 2 && (k == P.k_pl_E || riz_t == P.k_pl_E);
@@ -500,7 +502,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
         // a sheet plane through this position (both sheet loops below act
         // only there)
         bool sheet_here = false;
-        for (int s = 0; s < P.nsheet; s++) {
+        for (int s = 0; s < NS; s++) {
             const AemSheetPlane& S = P.sheet[s];
             sheet_here |= (S.axis == 0 ? px : S.axis == 1 ? py : pz) == S.pos;
         }
@@ -532,7 +534,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
             e = ga * eold + gb * curl;
 
             // sheet sub-cell field of the normal component, ref :5714-5780
-            for (int s = 0; sheet_here && s < P.nsheet; s++) {
+            for (int s = 0; sheet_here && s < NS; s++) {
                 const AemSheetPlane& S = P.sheet[s];
                 if (S.axis != comp) continue;
                 const int pn = comp == 0 ? px : comp == 1 ? py : pz;
@@ -646,20 +648,32 @@ int launch_update_h(const AemParams& Pin, int counter, cudaStream_t s) {
     AemParams P = Pin;
     upd_shape(P.zch_h, P.ty_h);
     dim3 blk(32, P.ty_h), grd((P.SX + 31) / 32, (P.SY + P.ty_h - 1) / P.ty_h, (P.SZ + P.zch_h - 1) / P.zch_h);
-    if (P.kmax) k_update_h<cf><<<grd, blk, 0, s>>>(P, counter);
-    else k_update_h<float><<<grd, blk, 0, s>>>(P, counter);
+    const bool sh = P.nsheet > 0;
+    if (P.kmax) {
+        if (sh) k_update_h<cf, true><<<grd, blk, 0, s>>>(P, counter);
+        else k_update_h<cf, false><<<grd, blk, 0, s>>>(P, counter);
+    } else {
+        if (sh) k_update_h<float, true><<<grd, blk, 0, s>>>(P, counter);
+        else k_update_h<float, false><<<grd, blk, 0, s>>>(P, counter);
+    }
     return 1;
 }
+template <typename T, bool DRUDE>
+static void launch_e(const AemParams& P, int counter, dim3 grd, dim3 blk, cudaStream_t s) {
+    if (P.nsheet > 0) k_update_e<T, DRUDE, true><<<grd, blk, 0, s>>>(P, counter);
+    else k_update_e<T, DRUDE, false><<<grd, blk, 0, s>>>(P, counter);
+}
+
 int launch_update_e(const AemParams& Pin, int counter, cudaStream_t s) {
     AemParams P = Pin;
     upd_shape(P.zch_e, P.ty_e);
     dim3 blk(32, P.ty_e), grd((P.SX + 31) / 32, (P.SY + P.ty_e - 1) / P.ty_e, (P.SZ + P.zch_e - 1) / P.zch_e);
     if (P.kmax) {
-        if (P.has_drude) k_update_e<cf, true><<<grd, blk, 0, s>>>(P, counter);
-        else k_update_e<cf, false><<<grd, blk, 0, s>>>(P, counter);
+        if (P.has_drude) launch_e<cf, true>(P, counter, grd, blk, s);
+        else launch_e<cf, false>(P, counter, grd, blk, s);
     } else {
-        if (P.has_drude) k_update_e<float, true><<<grd, blk, 0, s>>>(P, counter);
-        else k_update_e<float, false><<<grd, blk, 0, s>>>(P, counter);
+        if (P.has_drude) launch_e<float, true>(P, counter, grd, blk, s);
+        else launch_e<float, false>(P, counter, grd, blk, s);
     }
     return 1;
 }
