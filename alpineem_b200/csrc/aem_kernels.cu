@@ -56,6 +56,98 @@ __device__ inline T cpml_term(const AemParams& P, void* psi, float b, float c, T
 // of 8 rows; Solver::autotune times the candidates on a run's own steps.
 constexpr int UPD_ZCH = 16, UPD_TY = 8;
 
+// TF/SF corrections of one H position (FP32 runs), ref :4627-4794
+// (incident then mirrored); i, j, k reference indices
+__device__ __forceinline__ void tfsf_h(const AemParams& P, int i, int j, int k, float cntH, float& hxv, float& hyv,
+                                      float& hzv) {
+    if (P.tfsf_on) {  // TF/SF faces, ref :4627-4794 (incident then mirrored)
+        const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
+        for (int m = 0; m <= P.mirror_on; m++) {
+            const float wEx = P.WE[m][0], wEy = P.WE[m][1], wEz = P.WE[m][2];
+            if (!P.per[1]) {
+                const float cf_ = P.coef_h[1];
+                if (j == yl - 1 || j == yh) {
+                    const float yy = (float)(j == yh ? yh : yl), w = j == yh ? P.wall_hi[1] : P.wall_lo[1];
+                    const float sg = j == yh ? 1.0f : -1.0f;
+                    if (k >= zl && k <= zh && i >= xl && i <= xh - 1 + P.per[0])
+                        hzv = sg > 0 ? hzv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w
+                                     : hzv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w;
+                    if (k >= zl && k <= zh - 1 + P.per[2] && i >= xl && i <= xh)
+                        hxv = sg > 0 ? hxv - cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w
+                                     : hxv + cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w;
+                }
+            }
+            if (!P.per[2]) {
+                const float cf_ = P.coef_h[2];
+                if (k == zl - 1 || k == zh) {
+                    const float zz = (float)(k == zh ? zh : zl), w = k == zh ? P.wall_hi[2] : P.wall_lo[2];
+                    const bool hiface = k == zh;
+                    if (j >= yl && j <= yh && i >= xl && i <= xh - 1 + P.per[0])
+                        hyv = hiface ? hyv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w
+                                     : hyv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w;
+                    if (j >= yl && j <= yh - 1 + P.per[1] && i >= xl && i <= xh)
+                        hxv = hiface ? hxv + cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w
+                                     : hxv - cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w;
+                }
+            }
+            if (!P.per[0]) {
+                const float cf_ = P.coef_h[0];
+                if (i == xl - 1 || i == xh) {
+                    const float xx = (float)(i == xh ? xh : xl), w = i == xh ? P.wall_hi[0] : P.wall_lo[0];
+                    const bool hiface = i == xh;
+                    if (k >= zl && k <= zh && j >= yl && j <= yh - 1 + P.per[1])
+                        hzv = hiface ? hzv - cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w
+                                     : hzv + cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w;
+                    if (k >= zl && k <= zh - 1 + P.per[2] && j >= yl && j <= yh)
+                        hyv = hiface ? hyv + cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w
+                                     : hyv - cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w;
+                }
+            }
+        }
+    }
+}
+
+// TF/SF correction of E component comp (FP32 runs), ref :5950-6117; ri, rj,
+// rk the component's representative reference indices
+__device__ __forceinline__ void tfsf_e(const AemParams& P, int comp, int ri, int rj, int rk, float cntE, float& e) {
+    if (P.tfsf_on) {  // TF/SF faces, ref :5950-6117
+        const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
+        const int pbx = P.per[0], pby = P.per[1], pbz = P.per[2];
+        for (int m = 0; m <= P.mirror_on; m++) {
+            const float wHx = P.WH[m][0], wHy = P.WH[m][1], wHz = P.WH[m][2];
+            const float cy = P.coef_e[1], cz = P.coef_e[2], cx = P.coef_e[0];
+            if (comp == 0) {
+                if (!pby && (rj == yl || rj == yh) && rk >= zl + pbz && rk <= zh && ri >= xl && ri <= xh - 1 + pbx) {
+                    if (rj == yl) e = e - cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yl - 0.5f, (float)rk, cntE) * P.wall_lo[1];
+                    else e = e + cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yh + 0.5f, (float)rk, cntE) * P.wall_hi[1];
+                }
+                if (!pbz && (rk == zl || rk == zh) && rj >= yl + pby && rj <= yh && ri >= xl && ri <= xh - 1 + pbx) {
+                    if (rk == zl) e = e + cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zl - 0.5f, cntE) * P.wall_lo[2];
+                    else e = e - cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zh + 0.5f, cntE) * P.wall_hi[2];
+                }
+            } else if (comp == 1) {
+                if (!pbz && (rk == zl || rk == zh) && rj >= yl && rj <= yh - 1 + pby && ri >= xl + pbx && ri <= xh) {
+                    if (rk == zl) e = e - cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zl - 0.5f, cntE) * P.wall_lo[2];
+                    else e = e + cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zh + 0.5f, cntE) * P.wall_hi[2];
+                }
+                if (!pbx && (ri == xl || ri == xh) && rk >= zl + pbz && rk <= zh && rj >= yl && rj <= yh - 1 + pby) {
+                    if (ri == xl) e = e + cx * d_inc(P, m, wHz, (float)xl - 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_lo[0];
+                    else e = e - cx * d_inc(P, m, wHz, (float)xh + 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_hi[0];
+                }
+            } else {
+                if (!pby && (rj == yl || rj == yh) && rk >= zl && rk <= zh - 1 + pbz && ri >= xl + pbx && ri <= xh) {
+                    if (rj == yl) e = e + cy * d_inc(P, m, wHx, (float)ri, (float)yl - 0.5f, (float)rk + 0.5f, cntE) * P.wall_lo[1];
+                    else e = e - cy * d_inc(P, m, wHx, (float)ri, (float)yh + 0.5f, (float)rk + 0.5f, cntE) * P.wall_hi[1];
+                }
+                if (!pbx && (ri == xl || ri == xh) && rk >= zl && rk <= zh - 1 + pbz && rj >= yl + pby && rj <= yh) {
+                    if (ri == xl) e = e - cx * d_inc(P, m, wHy, (float)xl - 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_lo[0];
+                    else e = e + cx * d_inc(P, m, wHy, (float)xh + 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_hi[0];
+                }
+            }
+        }
+    }
+}
+
 // One thread per (x, y) column marching its z chunk.  The per-cell work
 // every position shares (bulk curl, CPML psi terms, periodic wraps) is
 // straight-line code with per-lane predicates, so lanes in a CPML slab or
@@ -64,7 +156,7 @@ constexpr int UPD_ZCH = 16, UPD_TY = 8;
 // flag per position, made of a column test done once and a plane test
 // done per plane.  E(k+1) stays in registers as the next plane's E(k).
 // The complex instantiation runs at 3 CTAs per SM (no spills).
-template <typename T, bool SHEETS>
+template <typename T, bool SHEETS, bool TFSF>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_update_h(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int NS = SHEETS ? P.nsheet : 0;  // decks without sheets compile the sheet code out
@@ -100,7 +192,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
     bool col_rare = false;
     for (int s = 0; s < NS; s++)
         col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
-    if (sizeof(T) == sizeof(float) && P.tfsf_on)
+    if (TFSF && P.tfsf_on)
         col_rare |= (!P.per[0] && (i == P.lo[0] - 1 || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] - 1 || j == P.hi[1]));
     if (sizeof(T) != sizeof(float) && P.kmax_mode_TE)
         col_rare |= (P.kmax_src_axis == 0 && i == P.k_pl_H) || (P.kmax_src_axis == 1 && j == P.k_pl_H);
@@ -130,7 +222,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
         const T ez_jp = ld_up<T>(P, Ez, c + offy, wy, 1);
         bool rare = col_rare;
         for (int s = 0; s < NS; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
-        if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] - 1 || k == P.hi[2]);
+        if (TFSF && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] - 1 || k == P.hi[2]);
         if (sizeof(T) != sizeof(float) && P.kmax_mode_TE) rare |= P.kmax_src_axis == 2 && k == P.k_pl_H;
 
         T hxv = ld<T>(Hx, c), hyv = ld<T>(Hy, c), hzv = ld<T>(Hz, c);
@@ -176,51 +268,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 5 : 3) k_upd
 
         // incident fields on H
         if constexpr (sizeof(T) == sizeof(float)) {
-            if (P.tfsf_on) {  // TF/SF faces, ref :4627-4794 (incident then mirrored)
-                const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
-                for (int m = 0; m <= P.mirror_on; m++) {
-                    const float wEx = P.WE[m][0], wEy = P.WE[m][1], wEz = P.WE[m][2];
-                    if (!P.per[1]) {
-                        const float cf_ = P.coef_h[1];
-                        if (j == yl - 1 || j == yh) {
-                            const float yy = (float)(j == yh ? yh : yl), w = j == yh ? P.wall_hi[1] : P.wall_lo[1];
-                            const float sg = j == yh ? 1.0f : -1.0f;
-                            if (k >= zl && k <= zh && i >= xl && i <= xh - 1 + P.per[0])
-                                hzv = sg > 0 ? hzv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w
-                                             : hzv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, yy, (float)k, cntH) * w;
-                            if (k >= zl && k <= zh - 1 + P.per[2] && i >= xl && i <= xh)
-                                hxv = sg > 0 ? hxv - cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w
-                                             : hxv + cf_ * d_inc(P, m, wEz, (float)i, yy, (float)k + 0.5f, cntH) * w;
-                        }
-                    }
-                    if (!P.per[2]) {
-                        const float cf_ = P.coef_h[2];
-                        if (k == zl - 1 || k == zh) {
-                            const float zz = (float)(k == zh ? zh : zl), w = k == zh ? P.wall_hi[2] : P.wall_lo[2];
-                            const bool hiface = k == zh;
-                            if (j >= yl && j <= yh && i >= xl && i <= xh - 1 + P.per[0])
-                                hyv = hiface ? hyv - cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w
-                                             : hyv + cf_ * d_inc(P, m, wEx, (float)i + 0.5f, (float)j, zz, cntH) * w;
-                            if (j >= yl && j <= yh - 1 + P.per[1] && i >= xl && i <= xh)
-                                hxv = hiface ? hxv + cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w
-                                             : hxv - cf_ * d_inc(P, m, wEy, (float)i, (float)j + 0.5f, zz, cntH) * w;
-                        }
-                    }
-                    if (!P.per[0]) {
-                        const float cf_ = P.coef_h[0];
-                        if (i == xl - 1 || i == xh) {
-                            const float xx = (float)(i == xh ? xh : xl), w = i == xh ? P.wall_hi[0] : P.wall_lo[0];
-                            const bool hiface = i == xh;
-                            if (k >= zl && k <= zh && j >= yl && j <= yh - 1 + P.per[1])
-                                hzv = hiface ? hzv - cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w
-                                             : hzv + cf_ * d_inc(P, m, wEy, xx, (float)j + 0.5f, (float)k, cntH) * w;
-                            if (k >= zl && k <= zh - 1 + P.per[2] && j >= yl && j <= yh)
-                                hyv = hiface ? hyv + cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w
-                                             : hyv - cf_ * d_inc(P, m, wEz, xx, (float)j, (float)k + 0.5f, cntH) * w;
-                        }
-                    }
-                }
-            }
+            if constexpr (TFSF) tfsf_h(P, i, j, k, cntH, hxv, hyv, hzv);
         } else {
             if (P.kmax_mode_TE) {  // kmax TE plane on H, ref :4562-4624
                 const int a = P.kmax_src_axis;
@@ -380,7 +428,7 @@ __device__ inline bool in_box(const AemParams& P, int c, int ri, int rj, int rk)
 // from the previous plane (FP32; the complex kernel reloads them and runs
 // 3 CTAs per SM without Drude poles, which overlaps better in a batch of
 // constant-k runs: 0.79 s against 1.00 s at 2 CTAs for 64 unit cells).
-template <typename T, bool DRUDE, bool SHEETS>
+template <typename T, bool DRUDE, bool SHEETS, bool TFSF>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ? 2 : 3)) k_update_e(const __grid_constant__ AemParams P, int counter) {
     counter = step_of(P, counter);
     const int NS = SHEETS ? P.nsheet : 0;  // decks without sheets compile the sheet code out
@@ -424,7 +472,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
     bool col_rare = false;
     for (int s = 0; s < NS; s++)
         col_rare |= (P.sheet[s].axis == 0 && px == P.sheet[s].pos) || (P.sheet[s].axis == 1 && py == P.sheet[s].pos);
-    if (sizeof(T) == sizeof(float) && P.tfsf_on)
+    if (TFSF && P.tfsf_on)
         col_rare |= (!P.per[0] && (i == P.lo[0] || i == P.hi[0])) || (!P.per[1] && (j == P.lo[1] || j == P.hi[1]));
     if (sizeof(T) != sizeof(float) && P.kmax_mode_TM)
         col_rare |= (P.kmax_src_axis == 0 && (i == P.k_pl_E || rix_t == P.k_pl_E)) ||
@@ -490,7 +538,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
         have = sizeof(T) == sizeof(float) && !unavg;  // the ids of this plane were read (FP32 only, as in H)
         bool rare = col_rare;
         for (int s = 0; s < NS; s++) rare |= P.sheet[s].axis == 2 && pz == P.sheet[s].pos;
-        if (sizeof(T) == sizeof(float) && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] || k == P.hi[2]);
+        if (TFSF && P.tfsf_on) rare |= !P.per[2] && (k == P.lo[2] || k == P.hi[2]);
         if (sizeof(T) != sizeof(float) && P.kmax_mode_TM)
             rare |= P.kmax_src_axis == 2 && (k == P.k_pl_E || riz_t == P.k_pl_E);
         if (col_drude)
@@ -550,42 +598,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
             if (DRUDE && P.has_drude && in_box(P, comp, ri, rj, rk)) e = drude_update<T>(P, comp, px, py, pz, e, eold, gb, co);
 
             if constexpr (sizeof(T) == sizeof(float)) {
-                if (P.tfsf_on) {  // TF/SF faces, ref :5950-6117
-                    const int xl = P.lo[0], xh = P.hi[0], yl = P.lo[1], yh = P.hi[1], zl = P.lo[2], zh = P.hi[2];
-                    const int pbx = P.per[0], pby = P.per[1], pbz = P.per[2];
-                    for (int m = 0; m <= P.mirror_on; m++) {
-                        const float wHx = P.WH[m][0], wHy = P.WH[m][1], wHz = P.WH[m][2];
-                        const float cy = P.coef_e[1], cz = P.coef_e[2], cx = P.coef_e[0];
-                        if (comp == 0) {
-                            if (!pby && (rj == yl || rj == yh) && rk >= zl + pbz && rk <= zh && ri >= xl && ri <= xh - 1 + pbx) {
-                                if (rj == yl) e = e - cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yl - 0.5f, (float)rk, cntE) * P.wall_lo[1];
-                                else e = e + cy * d_inc(P, m, wHz, (float)ri + 0.5f, (float)yh + 0.5f, (float)rk, cntE) * P.wall_hi[1];
-                            }
-                            if (!pbz && (rk == zl || rk == zh) && rj >= yl + pby && rj <= yh && ri >= xl && ri <= xh - 1 + pbx) {
-                                if (rk == zl) e = e + cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zl - 0.5f, cntE) * P.wall_lo[2];
-                                else e = e - cz * d_inc(P, m, wHy, (float)ri + 0.5f, (float)rj, (float)zh + 0.5f, cntE) * P.wall_hi[2];
-                            }
-                        } else if (comp == 1) {
-                            if (!pbz && (rk == zl || rk == zh) && rj >= yl && rj <= yh - 1 + pby && ri >= xl + pbx && ri <= xh) {
-                                if (rk == zl) e = e - cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zl - 0.5f, cntE) * P.wall_lo[2];
-                                else e = e + cz * d_inc(P, m, wHx, (float)ri, (float)rj + 0.5f, (float)zh + 0.5f, cntE) * P.wall_hi[2];
-                            }
-                            if (!pbx && (ri == xl || ri == xh) && rk >= zl + pbz && rk <= zh && rj >= yl && rj <= yh - 1 + pby) {
-                                if (ri == xl) e = e + cx * d_inc(P, m, wHz, (float)xl - 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_lo[0];
-                                else e = e - cx * d_inc(P, m, wHz, (float)xh + 0.5f, (float)rj + 0.5f, (float)rk, cntE) * P.wall_hi[0];
-                            }
-                        } else {
-                            if (!pby && (rj == yl || rj == yh) && rk >= zl && rk <= zh - 1 + pbz && ri >= xl + pbx && ri <= xh) {
-                                if (rj == yl) e = e + cy * d_inc(P, m, wHx, (float)ri, (float)yl - 0.5f, (float)rk + 0.5f, cntE) * P.wall_lo[1];
-                                else e = e - cy * d_inc(P, m, wHx, (float)ri, (float)yh + 0.5f, (float)rk + 0.5f, cntE) * P.wall_hi[1];
-                            }
-                            if (!pbx && (ri == xl || ri == xh) && rk >= zl && rk <= zh - 1 + pbz && rj >= yl + pby && rj <= yh) {
-                                if (ri == xl) e = e - cx * d_inc(P, m, wHy, (float)xl - 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_lo[0];
-                                else e = e + cx * d_inc(P, m, wHy, (float)xh + 0.5f, (float)rj, (float)rk + 0.5f, cntE) * P.wall_hi[0];
-                            }
-                        }
-                    }
-                }
+                if constexpr (TFSF) tfsf_e(P, comp, ri, rj, rk, cntE, e);
             } else {
                 if (P.kmax_mode_TM) {  // kmax TM plane on E, ref :5861-5947
                     const int a = P.kmax_src_axis;
@@ -638,6 +651,136 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(float) ? 3 : (DRUDE ?
 }
 
 // ---------------------------------------------------------------------------
+// TF/SF corrections in their own kernels (FP32 runs whose TF/SF faces stay
+// clear of every CPML slab, P.tfsf_sep): the shell of the TF/SF box, each
+// position once, after the bulk pass of its field.  The reference applies
+// them after the bulk, sheet and Drude terms and before the CPML terms; no
+// CPML term reaches these positions, so adding them afterwards is the same
+// sequence of operations.  Per axis a the shell spans reference indices
+// r0..r1 (the whole axis when periodic) and its faces sit at f0, f1 (none
+// when periodic); group X takes the x faces, Y the y faces off them, Z the
+// rest.
+struct Shell {
+    int r0[3], n[3], f[3][2], nf[3];
+};
+__device__ inline bool shell_cell(const Shell& S, long long t, int idx[3]) {
+    const int nx = S.n[0], ny = S.n[1], nz = S.n[2];
+    const int mx = nx - S.nf[0], my = ny - S.nf[1];  // x / y positions off the faces
+    auto off = [&](int a, int q) {                    // q-th index of axis a that is not a face
+        int v = S.r0[a] + q;
+        for (int u = 0; u < S.nf[a]; u++)
+            if (v >= S.f[a][u]) v++;
+        return v;
+    };
+    long long gx = (long long)S.nf[0] * ny * nz, gy = (long long)S.nf[1] * mx * nz, gz = (long long)S.nf[2] * mx * my;
+    if (t < gx) {
+        idx[0] = S.f[0][t / ((long long)ny * nz)];
+        const long long r = t % ((long long)ny * nz);
+        idx[1] = S.r0[1] + (int)(r % ny);
+        idx[2] = S.r0[2] + (int)(r / ny);
+        return true;
+    }
+    t -= gx;
+    if (t < gy) {
+        idx[1] = S.f[1][t / ((long long)mx * nz)];
+        const long long r = t % ((long long)mx * nz);
+        idx[0] = off(0, (int)(r % mx));
+        idx[2] = S.r0[2] + (int)(r / mx);
+        return true;
+    }
+    t -= gy;
+    if (t < gz) {
+        idx[2] = S.f[2][t / ((long long)mx * my)];
+        const long long r = t % ((long long)mx * my);
+        idx[0] = off(0, (int)(r % mx));
+        idx[1] = off(1, (int)(r / mx));
+        return true;
+    }
+    return false;
+}
+
+__global__ void k_tfsf_h(const __grid_constant__ AemParams P, const Shell S, long long total, int counter) {
+    counter = step_of(P, counter);
+    const float cntH = (float)counter - 1.0f;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int idx[3];
+        if (!shell_cell(S, t, idx)) continue;
+        const long long c = lin(P, idx[0] - 1, idx[1] - 1, idx[2] - 1);
+        float* Hx = reinterpret_cast<float*>(P.H[0]);
+        float* Hy = reinterpret_cast<float*>(P.H[1]);
+        float* Hz = reinterpret_cast<float*>(P.H[2]);
+        float hx = Hx[c], hy = Hy[c], hz = Hz[c];
+        tfsf_h(P, idx[0], idx[1], idx[2], cntH, hx, hy, hz);
+        Hx[c] = hx;
+        Hy[c] = hy;
+        Hz[c] = hz;
+    }
+}
+
+__global__ void k_tfsf_e(const __grid_constant__ AemParams P, const Shell S, long long total, int counter) {
+    counter = step_of(P, counter);
+    const float cntE = (float)counter - 0.5f;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int idx[3];
+        if (!shell_cell(S, t, idx)) continue;
+        const int px = idx[0] - 1, py = idx[1] - 1, pz = idx[2] - 1;
+        // the components k_update_e updates here (ref :5670-5702)
+        auto upd = [&](int a, int p, bool normal) {
+            const int Sa = a == 0 ? P.SX : a == 1 ? P.SY : P.SZ;
+            if (P.per[a]) return true;
+            return normal ? (p <= Sa - 2) : (p >= 1 && p <= Sa - 2);
+        };
+        const bool u[3] = {upd(0, px, true) && upd(1, py, false) && upd(2, pz, false),
+                           upd(0, px, false) && upd(1, py, true) && upd(2, pz, false),
+                           upd(0, px, false) && upd(1, py, false) && upd(2, pz, true)};
+        const int rix_t = rep_idx(P, 0, px, true), riy_t = rep_idx(P, 1, py, true), riz_t = rep_idx(P, 2, pz, true);
+        const long long c = lin(P, px, py, pz);
+        for (int comp = 0; comp < 3; comp++) {
+            if (!u[comp]) continue;
+            float* Ec = reinterpret_cast<float*>(P.E[comp]);
+            float e = Ec[c];
+            const int ri = comp == 0 ? px + 1 : rix_t, rj = comp == 1 ? py + 1 : riy_t, rk = comp == 2 ? pz + 1 : riz_t;
+            tfsf_e(P, comp, ri, rj, rk, cntE, e);
+            Ec[c] = e;
+        }
+    }
+}
+
+// the shell of H (faces lo-1, hi) or E (faces lo, hi)
+static long long tfsf_shell(const AemParams& P, bool e, Shell& S) {
+    const int Sx[3] = {P.SX, P.SY, P.SZ};
+    long long cells = 1;
+    for (int a = 0; a < 3; a++) {
+        if (P.per[a]) {
+            S.r0[a] = 1;
+            S.n[a] = Sx[a];
+            S.nf[a] = 0;
+        } else {
+            const int f0 = e ? P.lo[a] : P.lo[a] - 1, f1 = P.hi[a];
+            S.r0[a] = f0;
+            S.n[a] = f1 - f0 + 1;
+            S.f[a][0] = f0;
+            S.f[a][1] = f1;
+            S.nf[a] = f1 > f0 ? 2 : 1;
+        }
+        if (S.n[a] <= 0) return 0;
+        cells *= S.n[a];
+    }
+    const long long mx = S.n[0] - S.nf[0], my = S.n[1] - S.nf[1];
+    return (long long)S.nf[0] * S.n[1] * S.n[2] + (long long)S.nf[1] * mx * S.n[2] + (long long)S.nf[2] * mx * my;
+}
+
+static int launch_tfsf(const AemParams& P, bool e, int counter, cudaStream_t s) {
+    Shell S{};
+    const long long total = tfsf_shell(P, e, S);
+    if (total <= 0) return 0;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+    if (e) k_tfsf_e<<<blocks, 256, 0, s>>>(P, S, total, counter);
+    else k_tfsf_h<<<blocks, 256, 0, s>>>(P, S, total, counter);
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
 // a launch shape the caller did not set takes the default
 static void upd_shape(int& zch, int& ty) {
     if (zch < 1) zch = UPD_ZCH;
@@ -649,19 +792,25 @@ int launch_update_h(const AemParams& Pin, int counter, cudaStream_t s) {
     upd_shape(P.zch_h, P.ty_h);
     dim3 blk(32, P.ty_h), grd((P.SX + 31) / 32, (P.SY + P.ty_h - 1) / P.ty_h, (P.SZ + P.zch_h - 1) / P.zch_h);
     const bool sh = P.nsheet > 0;
+    // TF/SF inside the update kernel unless its own kernel applies it
+    const bool tf = P.tfsf_on && !P.tfsf_sep;
     if (P.kmax) {
-        if (sh) k_update_h<cf, true><<<grd, blk, 0, s>>>(P, counter);
-        else k_update_h<cf, false><<<grd, blk, 0, s>>>(P, counter);
+        if (sh) k_update_h<cf, true, false><<<grd, blk, 0, s>>>(P, counter);
+        else k_update_h<cf, false, false><<<grd, blk, 0, s>>>(P, counter);
+    } else if (tf) {
+        if (sh) k_update_h<float, true, true><<<grd, blk, 0, s>>>(P, counter);
+        else k_update_h<float, false, true><<<grd, blk, 0, s>>>(P, counter);
     } else {
-        if (sh) k_update_h<float, true><<<grd, blk, 0, s>>>(P, counter);
-        else k_update_h<float, false><<<grd, blk, 0, s>>>(P, counter);
+        if (sh) k_update_h<float, true, false><<<grd, blk, 0, s>>>(P, counter);
+        else k_update_h<float, false, false><<<grd, blk, 0, s>>>(P, counter);
     }
+    if (!P.kmax && P.tfsf_on && P.tfsf_sep && P.cpml_split != 2) return 1 + launch_tfsf(P, false, counter, s);
     return 1;
 }
-template <typename T, bool DRUDE>
+template <typename T, bool DRUDE, bool TFSF>
 static void launch_e(const AemParams& P, int counter, dim3 grd, dim3 blk, cudaStream_t s) {
-    if (P.nsheet > 0) k_update_e<T, DRUDE, true><<<grd, blk, 0, s>>>(P, counter);
-    else k_update_e<T, DRUDE, false><<<grd, blk, 0, s>>>(P, counter);
+    if (P.nsheet > 0) k_update_e<T, DRUDE, true, TFSF><<<grd, blk, 0, s>>>(P, counter);
+    else k_update_e<T, DRUDE, false, TFSF><<<grd, blk, 0, s>>>(P, counter);
 }
 
 int launch_update_e(const AemParams& Pin, int counter, cudaStream_t s) {
@@ -669,11 +818,18 @@ int launch_update_e(const AemParams& Pin, int counter, cudaStream_t s) {
     upd_shape(P.zch_e, P.ty_e);
     dim3 blk(32, P.ty_e), grd((P.SX + 31) / 32, (P.SY + P.ty_e - 1) / P.ty_e, (P.SZ + P.zch_e - 1) / P.zch_e);
     if (P.kmax) {
-        if (P.has_drude) launch_e<cf, true>(P, counter, grd, blk, s);
-        else launch_e<cf, false>(P, counter, grd, blk, s);
+        if (P.has_drude) launch_e<cf, true, false>(P, counter, grd, blk, s);
+        else launch_e<cf, false, false>(P, counter, grd, blk, s);
     } else {
-        if (P.has_drude) launch_e<float, true>(P, counter, grd, blk, s);
-        else launch_e<float, false>(P, counter, grd, blk, s);
+        const bool tf = P.tfsf_on && !P.tfsf_sep;
+        if (P.has_drude) {
+            if (tf) launch_e<float, true, true>(P, counter, grd, blk, s);
+            else launch_e<float, true, false>(P, counter, grd, blk, s);
+        } else {
+            if (tf) launch_e<float, false, true>(P, counter, grd, blk, s);
+            else launch_e<float, false, false>(P, counter, grd, blk, s);
+        }
+        if (P.tfsf_on && P.tfsf_sep && P.cpml_split != 2) return 1 + launch_tfsf(P, true, counter, s);
     }
     return 1;
 }

@@ -301,6 +301,18 @@ void Solver::setup_params() {
         P.coef_h[a] = d.del_t / (mu0 * dl[a]);
         P.coef_e[a] = d.del_t / (ep0 * dl[a]);
     }
+    // TF/SF faces (H: lo-1 and hi, E: lo and hi, over lo-1..hi on the other
+    // axes) clear of every CPML slab: the corrections can follow the update
+    // in their own kernels, since no CPML term reaches those positions
+    P.tfsf_sep = 0;
+    if (P.tfsf_on) {
+        bool sep = true;
+        for (int a = 0; a < 3; a++) {
+            if (d.pbc[a]) { sep &= d.npml[a][0] == 0 && d.npml[a][1] == 0; continue; }
+            sep &= d.lo[a] - 1 >= d.npml[a][0] && d.hi[a] <= N[a] - d.npml[a][1] && d.lo[a] - 1 >= 1 && d.hi[a] >= d.lo[a];
+        }
+        P.tfsf_sep = sep && !getenv_flag("AEM_TFSF_INLINE") ? 1 : 0;  // the switch: for comparisons
+    }
     P.t_spread = d.t_spread;
     P.spread = d.spread;
     P.exp_half = std::exp(0.5f);

@@ -107,6 +107,7 @@ struct AemParams {
     float sheet_thick;
     // TF/SF plane wave (standard solver)
     int tfsf_on, mirror_on;
+    int tfsf_sep;  // the TF/SF faces stay clear of every CPML slab: corrected by their own kernels
     int lo[3], hi[3];
     float wall_lo[3], wall_hi[3];
     float t_spread, spread, exp_half, inv_c;
