@@ -62,6 +62,17 @@ __device__ __forceinline__ BinW ff_binw(float tf) {
     return r;
 }
 
+// h + (w dd + d) on both lanes of a pair, rounded as fmaf then an add:
+// packed FP32, one fma and one add for two histogram components
+__device__ __forceinline__ float2 ff_acc2(float2 h, float w, float dd0, float dd1, float d0, float d1) {
+    float2 r;
+    asm("{\n .reg .b64 wa, xa, ya, pa, t;\n mov.b64 wa, {%2, %2};\n mov.b64 xa, {%3, %4};\n mov.b64 ya, {%5, %6};\n"
+        " mov.b64 pa, {%7, %8};\n fma.rn.ftz.f32x2 t, wa, xa, ya;\n add.rn.ftz.f32x2 t, pa, t;\n mov.b64 {%0, %1}, t;\n}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(w), "f"(dd0), "f"(dd1), "f"(d0), "f"(d1), "f"(h.x), "f"(h.y));
+    return r;
+}
+
 __device__ __forceinline__ void face_of_tile(const FarFieldDev& F, long long tile, int& f, int& u0, int& v0, int& nb,
                                              int& nc) {
     f = 0;
@@ -212,10 +223,8 @@ __global__ void __launch_bounds__(BIN_WARPS * 32, 2) k_ff_bin_tiles(const __grid
 #pragma unroll
             for (int q = 0; q < AW; q++) {
                 if (!on[q]) continue;
-                pu[q].x += fmaf(wu[q], dd[0], d[0]);
-                pu[q].y += fmaf(wu[q], dd[1], d[1]);
-                pw[q].x += fmaf(ww[q], dd[2], d[2]);
-                pw[q].y += fmaf(ww[q], dd[3], d[3]);
+                pu[q] = ff_acc2(pu[q], wu[q], dd[0], dd[1], d[0], d[1]);
+                pw[q] = ff_acc2(pw[q], ww[q], dd[2], dd[3], d[2], d[3]);
             }
 #pragma unroll
             for (int q = 0; q < AW; q++) {

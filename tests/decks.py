@@ -117,6 +117,22 @@ DECKS = {
                        objects=[("block", 4, (150, 20, 11), (1, 1, 5)), ("block", 4, (150, 20, 18), (1, 1, 5)),
                                 ("block", 5, (120, 14, 12), (20, 10, 12)), ("sphere", 5, (256, 20, 17), 5)],
                        ports=[("basic", "z", 50, (150, 20, 17), (1, 1, 1))]),
+    # x CPML 20 cells deep (sidecar pml_cells 19): the high x slab spans the
+    # seam between the second and third 128-cell tiles of the fused kernel,
+    # a lossy anisotropic block reaches into both x slabs and the y/z CPML
+    # corner
+    "fused_pml_edge": dict(n=(260, 52, 50), steps=120, f="15E9", pulse=1, excitation=("antenna", 1, 0, 1),
+                           ff=[(90, 0), (45, 120)], ffc=(130, 26, 25),
+                           mats=[("simple", 4, (1, 1, 1), ("1E8", "1E8", "1E8")), ("simple", 5, (4, 3, 2), (0.01, 0, 0))],
+                           objects=[("block", 4, (130, 26, 20), (1, 1, 5)), ("block", 4, (130, 26, 30), (1, 1, 5)),
+                                    ("block", 5, (5, 40, 12), (250, 6, 6))],
+                           ports=[("basic", "z", 50, (130, 26, 25), (1, 1, 1))], _ext="pml_cells 19\n"),
+    # CPML 23 cells deep (pml_cells 22) on every face
+    "fused_pml_deep": dict(n=(260, 60, 60), steps=120, f="15E9", pulse=1, excitation=("antenna", 1, 0, 1),
+                           ff=[(90, 0)], ffc=(130, 30, 30),
+                           mats=[("simple", 5, (4, 3, 2), (0.01, 0, 0))],
+                           objects=[("block", 5, (5, 44, 16), (250, 6, 6))],
+                           ports=[("basic", "z", 50, (130, 30, 30), (1, 1, 1))], _ext="pml_cells 22\n"),
     # the throughput workload at 48^3: bulk-file ellipsoids, 6-cell CPML
     # (sidecar), a 1-cell port and 56 far-field angles
     "ellipsoids_small": "ellipsoids_small",

@@ -4,7 +4,7 @@ x- or y-periodic ones) against the general two-kernel update
 reference's statements in its order in FP32, so every field must agree bit
 for bit, on every deck the fused kernels take (ports, CPML on six faces,
 material interfaces across tile seams, bulk-file ellipsoids, x- and
-z-periodic grids, chunk boundaries in z), at an odd step inside the run and
+z-periodic grids, chunk boundaries in z, CPML slabs up to 23 cells deep), at an odd step inside the run and
 at its end."""
 import numpy as np
 import pytest
@@ -14,7 +14,7 @@ import decks
 pytestmark = pytest.mark.gpu
 
 FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
-FUSED = ["dipole_port", "fused_wide", "ellipsoids_small", "dipole_pbc_x", "fused_long_z"]
+FUSED = ["dipole_port", "fused_wide", "ellipsoids_small", "dipole_pbc_x", "fused_long_z", "fused_pml_edge", "fused_pml_deep"]
 
 
 def _fields(name, d, monkeypatch, two_kernel, steps):
