@@ -399,7 +399,10 @@ def config_runs(max_over_ranks, world):
     configurations, each run whole on the device: Mcell-updates/s of all
     its steps (CUDA events on the solver's stream, every rank a replica),
     the per-phase split, and the update kernels' HBM roofline (the
-    algorithmic bytes of the Yee/CPML update over their summed event time)."""
+    algorithmic bytes of the Yee/CPML update over their summed event time);
+    then the same run again through CUDA-graph replay, timed by events
+    around the whole run (no per-phase events)."""
+    import torch
     import alpineem_b200 as ab
     from alpineem_b200 import workloads
     from alpineem_b200.deck import deck_text
@@ -421,11 +424,28 @@ def config_runs(max_over_ranks, world):
         sim.profile(False)
         shape = sim.autotune(0)  # the shapes the run tuned (no further steps)
         sim.close()
+        # the same run through CUDA-graph replay (aem_run_graph, 64-step
+        # graphs after the tuning steps), unprofiled: CUDA events on the
+        # solver's stream around the whole run, and the host clock
+        sim = ab.Simulation(deck_text=deck_text(deck), ext_text=ext + "autotune 2\n", outdir=tmp)
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        sim.run_graph(steps, 64)
+        ev1.record(stream)
+        sim.synchronize()
+        gwall = max_over_ranks(time.perf_counter() - t0)
+        gdev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        sim.close()
         dev_ms = max_over_ranks(sum(v[0] for v in prof.values()))
         t_upd = (prof["update_h"][0] + prof["update_e"][0] + prof["yee"][0]) / steps / 1e3
         out[name] = {"grid": list(deck["n"]), "steps": steps, "cells": cells,
                      "device_mcell_updates_per_s": round(world * cells * steps / (dev_ms / 1e3) / 1e6, 1),
                      "wall_mcell_updates_per_s": round(world * cells * steps / wall / 1e6, 1),
+                     "graph_device_mcell_updates_per_s": round(world * cells * steps / gdev / 1e6, 1),
+                     "graph_wall_mcell_updates_per_s": round(world * cells * steps / gwall / 1e6, 1),
                      "phases_ms_per_step": {k: round(v[0] / steps, 5) for k, v in prof.items() if v[1]},
                      "update_roofline_frac": round(bytes_step / t_upd / 1e9 / peak, 4),
                      "update_path": "fused k_yee4" if prof["yee"][1] else "k_update_h + k_update_e",
